@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 NUFFT engine (one JSON line on rank 0).
+
+Workload (default ``c2``): 3D type-2 + type-1 round pair, M = 1e7 points i.i.d. uniform in
+[-pi, pi)^3 (float32), N = 128^3 complex64 modes N(0,1), complex64 strengths N(0,1), tol 1e-6,
+upsampfac 2 (fine grid 256^3). Synthetic, seeded data; no public dataset is involved.
+
+One step = set_points (binning) + transform_type_2 + transform_type_1 on the same points, so
+the metric, NU points per second per transform, is 2 M / step time (set_points included).
+``--workload ns`` runs the 3D type-1 case M = 1e8, N = 256^3 (step = set_points + type 1).
+
+Timing: W untimed warm-up steps, then K steps between CUDA events on the plan's stream,
+bracketed by barrier + synchronize, max over ranks. The inputs (coordinates 120 MB, strengths
+80 MB, modes 17 MB, fine grid 134 MB) exceed the 126 MB L2, so no extra flush is done.
+
+Multi-GPU: the path does not shard a single transform; ranks run independent replicas
+(weak scaling, no data-path collective) and ``value`` sums the points of all ranks.
+
+``--impl reference`` times the reference's CPU path restated in oracle/ (the reference CPU
+library needs FFTW and Google Highway, absent here) on the host cores, on a bounded sample of
+the same workload per step; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "c2": dict(name="3D type-2 + type-1 round pair, M=1e7 uniform [-pi,pi)^3, N=128^3, tol 1e-6",
+               dim=3, M=10_000_000, N=128, tol=1e-6, types=(2, 1), seed=2, cpu_sample=1_000_000),
+    "ns": dict(name="3D type-1, M=1e8 uniform [-pi,pi)^3, N=256^3, tol 1e-6",
+               dim=3, M=100_000_000, N=256, tol=1e-6, types=(1,), seed=7, cpu_sample=1_000_000),
+    "c1": dict(name="2D type-1, M=1e5 uniform [-pi,pi)^2, N=256^2, tol 1e-6",
+               dim=2, M=100_000, N=256, tol=1e-6, types=(1,), seed=1, cpu_sample=100_000),
+}
+METRIC = "NU points/sec per transform at rel-l2 <=1e-6 (tuned FP32 vs plain GPU; CPU ref)"
+UNIT = "points/s"
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_port_step(wl, M, workers):
+    """One step of the restated reference CPU path (oracle) on M points of the workload."""
+    import numpy as np
+    from oracle import oracle as O
+    rng = np.random.default_rng(wl["seed"] + 1000)
+    dim, N = wl["dim"], wl["N"]
+    x = [rng.uniform(-np.pi, np.pi, M).astype(np.float32) for _ in range(dim)]
+    c = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+    f = (rng.standard_normal(N ** dim) + 1j * rng.standard_normal(N ** dim)).astype(np.complex64)
+    t0 = time.perf_counter()
+    plan = O.RefPlan(np.float32, -1, x, [N] * dim, tol=wl["tol"], workers=workers)
+    for t in wl["types"]:
+        if t == 2:
+            plan.transform_type_2(f)
+        else:
+            plan.transform_type_1(c)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, wl):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    M = wl["cpu_sample"]
+    for _ in range(args.warmup):
+        cpu_port_step(wl, M, cores)
+    ts = [cpu_port_step(wl, M, cores) for _ in range(args.steps)]
+    t = sum(ts) / len(ts)
+    ntr = len(wl["types"])
+    value = ntr * M / t
+    sample = (f"{M} of the workload's {wl['M']} points per step, same grid and tolerance; "
+              "spread serial and interpolation threaded as in the reference CPU plan, FFT by scipy")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform points, N(0,1) strengths)",
+        "config": {"workload": wl["name"], "M": wl["M"], "N": wl["N"], "dim": wl["dim"],
+                   "tol": wl["tol"], "sample_points": M},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--samples", type=int, default=10000)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import neonufft_b200 as nnb
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    dim, M, N, tol = wl["dim"], wl["M"], wl["N"], wl["tol"]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(wl["seed"] + 97 * rank)
+    loc = [(torch.rand(M, generator=g, device="cuda", dtype=torch.float32) * 2 - 1) * math.pi
+           for _ in range(dim)]
+    c = torch.complex(torch.randn(M, generator=g, device="cuda"),
+                      torch.randn(M, generator=g, device="cuda"))
+    nm = N ** dim
+    f = torch.complex(torch.randn(nm, generator=g, device="cuda"),
+                      torch.randn(nm, generator=g, device="cuda"))
+    out1 = torch.empty(nm, dtype=torch.complex64, device="cuda")
+    out2 = torch.empty(M, dtype=torch.complex64, device="cuda")
+    strides = [1, N, N * N][:dim]
+    modes = [N] * dim
+    opt = nnb.Options(tol=tol)
+    plan = nnb.Plan(opt, -1, M, loc, modes)
+    info = plan.info()
+
+    def step(lc, ff, cc, o2, o1):
+        plan.set_points(M, lc)
+        for t in wl["types"]:
+            if t == 2:
+                plan.transform_type_2(ff, strides, o2)
+            else:
+                plan.transform_type_1(cc, o1, strides)
+
+    for _ in range(args.warmup):
+        step(loc, f, c, out2, out1)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing ------------------------------------------------------------
+    clocks = ClockSampler(local)
+    plan.enable_timing(True)
+    plan.stage_times(reset=True)
+    l0 = nnb.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step(loc, f, c, out2, out1)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = nnb.kernel_launches() - l0
+    stages = plan.stage_times(reset=True)
+    plan.enable_timing(False)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    ntr = len(wl["types"])
+    value = world * ntr * M / (ms_step * 1e-3)
+
+    # ---- end-to-end through the public API with host buffers --------------------------------
+    pin = dict(device="cpu", pin_memory=True)
+    loc_h = [torch.empty(M, dtype=torch.float32, **pin) for _ in range(dim)]
+    for a, b in zip(loc_h, loc):
+        a.copy_(b)
+    c_h = torch.empty(M, dtype=torch.complex64, **pin)
+    c_h.copy_(c)
+    f_h = torch.empty(nm, dtype=torch.complex64, **pin)
+    f_h.copy_(f)
+    o1_h = torch.empty(nm, dtype=torch.complex64, **pin)
+    o2_h = torch.empty(M, dtype=torch.complex64, **pin)
+    loc_d = [torch.empty_like(a) for a in loc]
+    c_d, f_d = torch.empty_like(c), torch.empty_like(f)
+    h2d = dim * M * 4 + (M * 8 if 1 in wl["types"] else 0) + (nm * 8 if 2 in wl["types"] else 0)
+    d2h = (nm * 8 if 1 in wl["types"] else 0) + (M * 8 if 2 in wl["types"] else 0)
+
+    def e2e_step():
+        for a, b in zip(loc_d, loc_h):
+            a.copy_(b, non_blocking=True)
+        if 1 in wl["types"]:
+            c_d.copy_(c_h, non_blocking=True)
+        if 2 in wl["types"]:
+            f_d.copy_(f_h, non_blocking=True)
+        step(loc_d, f_d, c_d, out2, out1)
+        if 1 in wl["types"]:
+            o1_h.copy_(out1, non_blocking=True)
+        if 2 in wl["types"]:
+            o2_h.copy_(out2, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * ntr * M / (ms_e2e / args.steps * 1e-3)
+
+    # ---- accuracy vs the FP64 direct sum on sampled outputs (not timed) ---------------------
+    acc = {}
+    if not args.no_accuracy:
+        S = min(args.samples, 65535)
+        gs = torch.Generator(device="cuda")
+        gs.manual_seed(123)
+        loc64 = [a.double() for a in loc]
+        if 1 in wl["types"]:
+            idx = torch.randint(0, nm, (S,), generator=gs, device="cuda")
+            kk = []
+            rem = idx.clone()
+            for d in range(dim):
+                kk.append(rem % N - N // 2)
+                rem = rem // N
+            kidx = torch.stack(kk, dim=1).contiguous()
+            ref = torch.empty(S, dtype=torch.complex128, device="cuda")
+            nnb.direct_type1_f64(-1, loc64, c.to(torch.complex128), kidx, ref)
+            got = out1[idx].to(torch.complex128)
+            acc["type1_rel_l2"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        if 2 in wl["types"]:
+            pidx = torch.randint(0, M, (S,), generator=gs, device="cuda")
+            ref = torch.empty(S, dtype=torch.complex128, device="cuda")
+            nnb.direct_type2_f64(-1, modes, f.to(torch.complex128), loc64, pidx, ref)
+            got = out2[pidx].to(torch.complex128)
+            acc["type2_rel_l2"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        acc["samples"] = S
+        torch.cuda.synchronize()
+
+    # ---- roofline of the dominant kernel -----------------------------------------------------
+    peak, peak_kind = load_peaks()
+    spread_ms = stages["spread"][0] / max(1, stages["spread"][1])
+    interp_ms = stages["interp"][0] / max(1, stages["interp"][1]) if stages["interp"][1] else 0.0
+    w = info["n_spread"]
+    nf_cells = int(np.prod(info["grid"][:dim]))
+    # algorithmic bytes of one spread launch: per point perm + packed cell + dim fractions
+    # (4 B each) + its complex64 strength, plus one write of the complex64 fine grid.
+    spread_bytes = M * (4 + 4 + 4 * dim + 8) + nf_cells * 8
+    spread_flop = M * 5 * w ** dim
+    dom = "spread"
+    dom_ms, dom_bytes, dom_flop = spread_ms, spread_bytes, spread_flop
+    if interp_ms > spread_ms:
+        dom = "interp"
+        dom_ms = interp_ms
+        dom_bytes = M * (4 + 4 + 4 * dim + 8) + nf_cells * 8
+        dom_flop = M * 5 * w ** dim
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    fp32_peak = 148 * 128 * 2 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
+    roofline = {
+        "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} HBM copy",
+        "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+        "fp32": {"achieved_tflops": dom_flop / (dom_ms * 1e-3) / 1e12,
+                 "peak_tflops_nominal": fp32_peak,
+                 "frac": dom_flop / (dom_ms * 1e-3) / 1e12 / fp32_peak,
+                 "flop_per_point": 5 * w ** dim},
+    }
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            cores = os.cpu_count() or 1
+            O.set_threads(cores)
+            Ms = wl["cpu_sample"]
+            tcpu = cpu_port_step(wl, Ms, cores)
+            cpu = {"value": ntr * Ms / tcpu, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"one step on {Ms} of the {M} points (same grid, tol), "
+                             f"{tcpu:.2f} s; restated reference CPU path (oracle/)"}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform points, N(0,1) strengths and modes)",
+            "config": {"workload": wl["name"], "M": M, "N": N, "dim": dim, "tol": tol,
+                       "upsampfac": 2.0, "n_spread": w, "fine_grid": info["grid"][:dim],
+                       "tile": info["tile"][:dim], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (126 MB); no flush"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

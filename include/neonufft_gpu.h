@@ -1,0 +1,265 @@
+/*
+ * neonufft_gpu.h -- C ABI of the B200 NUFFT engine (libneonufft_b200.so).
+ *
+ * This is the drop-in boundary for the GPU plan of NeoNUFFT. Every entry point takes plain
+ * pointers and sizes and returns a NeonufftError; nothing here depends on C++ or on torch.
+ * The C++ classes neonufft::gpu::Plan / neonufft::gpu::PlanT3 (include/neonufft/gpu/plan.hpp)
+ * are header-only shims over these functions, so C++ code written against the reference
+ * compiles and links against this library unchanged.
+ *
+ * Conventions shared by all entry points:
+ *  - All array pointers are DEVICE pointers owned by the caller, as in the reference
+ *    (reference include/neonufft/gpu/plan.hpp:30-41).
+ *  - Coordinates are passed as `dim` separate arrays (structure of arrays), `loc[d]` holding
+ *    the d-th coordinate of every point, of type float (NNB_FLOAT) or double (NNB_DOUBLE).
+ *  - Complex data is interleaved (cuComplex / cuDoubleComplex layout).
+ *  - Grids and mode arrays are column-major: dimension 0 varies fastest.
+ *  - Work is asynchronous on the plan's stream, except where noted (point setup synchronises,
+ *    as the reference does: src/neonufft/gpu/plan_impl.hpp:151).
+ *  - On failure the function returns an error code and nnb_last_error_message() describes it.
+ */
+#ifndef NEONUFFT_GPU_H
+#define NEONUFFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "neonufft/enums.h"
+#include "neonufft/errors.h"
+
+#if defined(__GNUC__)
+#define NNB_API __attribute__((visibility("default")))
+#else
+#define NNB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#else
+typedef enum NeonufftError NeonufftError;
+#endif
+
+/* Floating-point type of a plan (the reference instantiates T = float, double:
+ * src/neonufft/gpu/plan.cpp:47-53). */
+typedef enum NnbPrecision { NNB_FLOAT = 0, NNB_DOUBLE = 1 } NnbPrecision;
+
+/* Plan options. The first nine fields mirror neonufft::Options
+ * (reference include/neonufft/plan.hpp:19-29). The remaining fields are engine extensions;
+ * zero selects the automatic choice. */
+typedef struct NnbOptions {
+  double tol;
+  double upsampfac;
+  double recenter_threshold;
+  int num_threads;          /* ignored on the GPU, as in the reference */
+  int sort_input;           /* ignored: points are always bin-sorted */
+  int sort_output;          /* ignored: points are always bin-sorted */
+  int kernel_approximation; /* ignored: the ES kernel is always evaluated directly */
+  int order;                /* NeonufftModeOrder */
+  int kernel_type;          /* NeonufftKernelType */
+  int tile[3];              /* subproblem tile (bin) shape in fine-grid cells; 0 = automatic */
+  int spread_method;        /* 0 = automatic; see nnb_plan_info */
+  int reserved[8];
+} NnbOptions;
+
+/* Fills *opt with the reference defaults (tol 1e-3, upsampfac 2, recenter 0.1, CMCL). */
+NNB_API void nnb_options_default(NnbOptions* opt);
+
+/* Device allocator used for every buffer a plan owns. Mirrors neonufft::Allocator
+ * (reference include/neonufft/allocator.hpp:12-21) as two callbacks. A NULL allocator pointer
+ * or NULL callbacks select cudaMalloc / cudaFree (reference src/neonufft/gpu/device_allocator.cpp).
+ * `allocate` returns NULL to signal failure; the plan then fails with
+ * NEONUFFT_MEMORY_ALLOC_ERROR. */
+typedef void* (*NnbAllocateFn)(void* ctx, size_t size);
+typedef void (*NnbDeallocateFn)(void* ctx, void* ptr);
+typedef struct NnbAllocator {
+  NnbAllocateFn allocate;
+  NnbDeallocateFn deallocate;
+  void* ctx;
+} NnbAllocator;
+
+typedef struct NnbPlan_s* NnbPlan;
+typedef struct NnbPlanT3_s* NnbPlanT3;
+
+/* ---------------------------------------------------------------------------------------
+ * Type 1 / type 2 plan.
+ * ------------------------------------------------------------------------------------- */
+
+/* Creates a type-1/2 plan and sets its points.
+ * Replaces gpu::Plan<T,DIM>::Plan (reference include/neonufft/gpu/plan.hpp:30-32).
+ * dim in {1,2,3}; modes[d] >= 1; sign is the sign of the exponent; stream is a cudaStream_t
+ * (NULL = legacy default stream). Synchronises the stream. */
+NNB_API NeonufftError nnb_plan_create(NnbPlan* plan, NnbPrecision precision, int dim,
+                              const NnbOptions* opt, int sign, int64_t num_nu,
+                              const void* const* loc, const int64_t* modes, void* stream,
+                              const NnbAllocator* alloc);
+
+/* Replaces the point set. Replaces gpu::Plan<T,DIM>::set_points
+ * (reference include/neonufft/gpu/plan.hpp:41). Synchronises the stream. */
+NNB_API NeonufftError nnb_plan_set_points(NnbPlan plan, int64_t num_nu, const void* const* loc);
+
+/* Type 1: out[k] = sum_j in[j] exp(i*sign*k.x_j), k in the modes box, written with
+ * out_strides (in elements). Replaces gpu::Plan<T,DIM>::transform_type_1
+ * (reference include/neonufft/gpu/plan.hpp:34-35). */
+NNB_API NeonufftError nnb_plan_transform_type_1(NnbPlan plan, const void* in, void* out,
+                                        const int64_t* out_strides);
+
+/* Type 2: out[j] = sum_k in[k] exp(i*sign*k.x_j), in read with in_strides (in elements).
+ * Replaces gpu::Plan<T,DIM>::transform_type_2 (reference include/neonufft/gpu/plan.hpp:37-39). */
+NNB_API NeonufftError nnb_plan_transform_type_2(NnbPlan plan, const void* in, const int64_t* in_strides,
+                                        void* out);
+
+/* Destroys the plan and frees its buffers (reference pImpl deleter,
+ * src/neonufft/gpu/plan.cpp:16-21). Accepts NULL. */
+NNB_API NeonufftError nnb_plan_destroy(NnbPlan plan);
+
+/* ---------------------------------------------------------------------------------------
+ * Type 3 plan.
+ * ------------------------------------------------------------------------------------- */
+
+/* Device memory in bytes of the fine grids a type-3 plan with these bounds would allocate.
+ * Replaces gpu::PlanT3<T,DIM>::grid_memory_size (reference include/neonufft/gpu/plan.hpp:52-56).
+ * Bounds are passed as double; for NNB_FLOAT they are rounded to float first. */
+NNB_API NeonufftError nnb_plan_t3_grid_memory_size(NnbPrecision precision, int dim, const NnbOptions* opt,
+                                           const double* input_min, const double* input_max,
+                                           const double* output_min, const double* output_max,
+                                           uint64_t* size);
+
+/* Creates a type-3 plan from point sets (bounds computed on the device).
+ * Replaces gpu::PlanT3<T,DIM>::PlanT3(opt, sign, num_in, input_points, num_out, output_points,
+ * stream, batch_size, alloc) (reference include/neonufft/gpu/plan.hpp:58-61). Synchronises. */
+NNB_API NeonufftError nnb_plan_t3_create(NnbPlanT3* plan, NnbPrecision precision, int dim,
+                                 const NnbOptions* opt, int sign, int64_t num_in,
+                                 const void* const* input_points, int64_t num_out,
+                                 const void* const* output_points, void* stream,
+                                 int64_t batch_size, const NnbAllocator* alloc);
+
+/* Creates a type-3 plan from coordinate bounds; points are set later.
+ * Replaces gpu::PlanT3<T,DIM>::PlanT3(opt, sign, input_min, input_max, output_min, output_max,
+ * stream, batch_size, alloc) (reference include/neonufft/gpu/plan.hpp:63-66). */
+NNB_API NeonufftError nnb_plan_t3_create_bounds(NnbPlanT3* plan, NnbPrecision precision, int dim,
+                                        const NnbOptions* opt, int sign, const double* input_min,
+                                        const double* input_max, const double* output_min,
+                                        const double* output_max, void* stream,
+                                        int64_t batch_size, const NnbAllocator* alloc);
+
+/* Replaces gpu::PlanT3::set_input_points (reference include/neonufft/gpu/plan.hpp:68-69). */
+NNB_API NeonufftError nnb_plan_t3_set_input_points(NnbPlanT3 plan, int64_t num_in,
+                                           const void* const* input_points);
+
+/* Replaces gpu::PlanT3::set_output_points (reference include/neonufft/gpu/plan.hpp:71-72). */
+NNB_API NeonufftError nnb_plan_t3_set_output_points(NnbPlanT3 plan, int64_t num_out,
+                                            const void* const* output_points);
+
+/* Accumulates batch_size input vectors (batch b at in + b*bdist; bdist <= 0 means num_in).
+ * Replaces gpu::PlanT3::add_input (reference include/neonufft/gpu/plan.hpp:74). */
+NNB_API NeonufftError nnb_plan_t3_add_input(NnbPlanT3 plan, const void* in, int64_t bdist);
+
+/* Computes batch_size outputs (batch b at out + b*bdist; bdist <= 0 means num_out).
+ * Replaces gpu::PlanT3::transform (reference include/neonufft/gpu/plan.hpp:76). */
+NNB_API NeonufftError nnb_plan_t3_transform(NnbPlanT3 plan, void* out, int64_t bdist);
+
+/* Clears the accumulated input. Replaces gpu::PlanT3::reset
+ * (reference include/neonufft/gpu/plan.hpp:78). */
+NNB_API NeonufftError nnb_plan_t3_reset(NnbPlanT3 plan);
+
+/* Destroys a type-3 plan. Accepts NULL. */
+NNB_API NeonufftError nnb_plan_t3_destroy(NnbPlanT3 plan);
+
+/* ---------------------------------------------------------------------------------------
+ * Support.
+ * ------------------------------------------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" if none). */
+NNB_API const char* nnb_last_error_message(void);
+
+/* Default device allocator: neonufft::gpu::DeviceAllocator::allocate / deallocate
+ * (reference include/neonufft/gpu/device_allocator.hpp:14-21). */
+NNB_API NeonufftError nnb_device_alloc(void** ptr, size_t size);
+NNB_API NeonufftError nnb_device_free(void* ptr);
+
+/* Plan introspection (engine extension, no reference counterpart). */
+typedef struct NnbPlanInfo {
+  int dim;
+  int precision;       /* NnbPrecision */
+  int n_spread;        /* kernel width w */
+  int spread_method;   /* method actually used */
+  double es_beta;      /* ES kernel shape parameter (as used, i.e. rounded to T) */
+  int64_t grid[3];     /* FFT grid (fine grid) dims; 1 for unused dims */
+  int64_t spread_grid[3]; /* type 3: spread grid dims; type 1/2: equals grid */
+  int tile[3];         /* subproblem tile shape */
+  int64_t num_in;      /* points (type 1/2) or sources (type 3) */
+  int64_t num_out;     /* type 3 targets */
+  int64_t batch_size;
+  uint64_t device_bytes; /* bytes currently held through the allocator */
+  double input_offset[3], output_offset[3], gamma[3], h[3]; /* type 3 geometry */
+} NnbPlanInfo;
+NNB_API NeonufftError nnb_plan_info(NnbPlan plan, NnbPlanInfo* info);
+NNB_API NeonufftError nnb_plan_t3_info(NnbPlanT3 plan, NnbPlanInfo* info);
+
+/* Per-stage device timing (engine extension). When enabled, the plan records CUDA events on
+ * its stream around each stage; nnb_*_stage_times adds the elapsed milliseconds since the last
+ * reset into ms[NNB_STAGE_COUNT] (synchronises the stream) and launch counts into count[]. */
+enum NnbStage {
+  NNB_STAGE_BIN = 0,     /* point binning: rescale, count, scan, permutation */
+  NNB_STAGE_SPREAD = 1,  /* ES spreading kernel (the grid is zeroed just before, outside) */
+  NNB_STAGE_FFT = 2,     /* cuFFT */
+  NNB_STAGE_DECONV = 3,  /* deconvolution (downsample / upsample) */
+  NNB_STAGE_INTERP = 4,  /* ES interpolation */
+  NNB_STAGE_PHASE = 5,   /* type-3 pre/post phase and bounds */
+  NNB_STAGE_COUNT = 6
+};
+NNB_API NeonufftError nnb_plan_enable_timing(NnbPlan plan, int enable);
+NNB_API NeonufftError nnb_plan_stage_times(NnbPlan plan, double* ms, int64_t* count, int reset);
+NNB_API NeonufftError nnb_plan_t3_enable_timing(NnbPlanT3 plan, int enable);
+NNB_API NeonufftError nnb_plan_t3_stage_times(NnbPlanT3 plan, double* ms, int64_t* count, int reset);
+
+/* FP64 direct NUDFT on the GPU, for accuracy measurement (engine extension; the reference
+ * computes the same sums on the CPU in tests/nuft_direct_kernels.cpp:73-293).
+ * Coordinates and data are double; sampled outputs only:
+ *   type 1: out[s] = sum_j in[j] exp(i*sign*k_s.x_j) for the mode multi-indices k_s given in
+ *           modes_idx (num_samples x dim, int64, signed mode numbers);
+ *   type 2: out[s] = sum_k in[k] exp(i*sign*k.x_{p_s}) for the points p_s listed in point_idx,
+ *           modes in CMCL order, column-major, n_modes[d] per dim;
+ *   type 3: out[s] = sum_j in[j] exp(i*sign*s_{t}.x_j) for the targets listed in target_idx. */
+NNB_API NeonufftError nnb_direct_type1_f64(int dim, int sign, int64_t num_nu, const double* const* loc,
+                                   const double* in, int64_t num_samples, const int64_t* modes_idx,
+                                   double* out, void* stream);
+NNB_API NeonufftError nnb_direct_type2_f64(int dim, int sign, const int64_t* n_modes, const double* in,
+                                   const double* const* loc, int64_t num_samples,
+                                   const int64_t* point_idx, double* out, void* stream);
+NNB_API NeonufftError nnb_direct_type3_f64(int dim, int sign, int64_t num_in, const double* const* in_loc,
+                                   const double* in, const double* const* out_loc,
+                                   int64_t num_samples, const int64_t* target_idx, double* out,
+                                   void* stream);
+
+/* Host-only parameter queries (engine extensions; no GPU needed). They expose the engine's own
+ * restatement of the reference's heuristics so that sizing can be planned ahead:
+ *  - ES kernel width w, shape beta and c = 4/w^2 as used by a plan of this precision
+ *    (reference src/neonufft/es_kernel_param.hpp:24-56);
+ *  - type-3 geometry per dimension: spread grid nf1, FFT grid, input centre C, output centre D,
+ *    gamma and h (reference src/neonufft/util/grid_info_t3.hpp:18-52,
+ *    src/contrib/es_kernel/util.hpp:64-105);
+ *  - deconvolution factors (-1)^k / phi_hat(2 pi k / nf), k = 0..nf/2, in double. */
+NNB_API NeonufftError nnb_es_kernel_params(double tol, double upsampfac, NnbPrecision precision,
+                                           int* n_spread, double* beta, double* c);
+NNB_API NeonufftError nnb_plan_t3_geometry(NnbPrecision precision, int dim, const NnbOptions* opt,
+                                           const double* input_min, const double* input_max,
+                                           const double* output_min, const double* output_max,
+                                           int64_t* spread_grid, int64_t* fft_grid,
+                                           double* input_offset, double* output_offset,
+                                           double* gamma, double* h);
+NNB_API NeonufftError nnb_deconv_factors(double tol, double upsampfac, NnbPrecision precision,
+                                         int64_t nf, double* out);
+
+/* Library version string. */
+NNB_API const char* nnb_version(void);
+
+/* Number of engine kernels this process has launched so far (all plans and devices; cuFFT's
+ * kernels are not counted). Engine extension for launch accounting. */
+NNB_API int64_t nnb_kernel_launches(void);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* NEONUFFT_GPU_H */

@@ -1,0 +1,252 @@
+// Point binning: rescale, tile histogram, exclusive scan, permutation.
+//
+// Replaces the reference's rescale_and_permut (src/neonufft/gpu/kernels/rescale_loc_kernel.cu:23-126,
+// :185-209), which counts with one global atomic per point, assigns bin offsets from a single
+// block in atomic (non-deterministic) order and scatters 24-32 byte Point structs with a second
+// atomic per point. Here:
+//  - the rescaling runs in double precision for every plan precision, and the point is stored
+//    as its tile-local first kernel cell (packed integers) plus the fractional kernel argument
+//    i0 - loc, so single-precision plans keep the full double-precision position;
+//  - pass 1 records each point's rank inside its tile (the only atomic);
+//  - a three-kernel device-wide exclusive scan gives tile offsets in tile order;
+//  - pass 2 writes structure-of-arrays records (perm, local, frac[d]) with no atomics.
+#include "kernels.cuh"
+
+namespace nnb {
+
+namespace {
+
+constexpr int kBinBlock = 256;
+
+// First kernel cell of one coordinate: i0 = ceil(loc - w/2) wrapped to [0, nf), and the
+// kernel argument frac = i0 - loc in [-w/2, -w/2 + 1]. Returns false for non-finite input.
+__device__ __forceinline__ bool cell_of(const BinGeom& g, int d, double x, i64& i0w,
+                                        double& frac) {
+  const double v = (x - g.offset[d]) * g.scale[d];
+  double p = (v + kPi) * kTwoPiInv;
+  p = p - floor(p);
+  const double nf = double(g.nf[d]);
+  const double loc = p * nf;
+  const double s = ceil(loc - 0.5 * double(g.w));
+  frac = s - loc;
+  if (!(frac == frac) || !(fabs(frac) <= 16.0)) return false;
+  i64 i0 = static_cast<i64>(s);
+  const i64 n = g.nf[d];
+  while (i0 < 0) i0 += n;
+  while (i0 >= n) i0 -= n;
+  i0w = i0;
+  return true;
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kBinBlock)
+    bin_count_kernel(BinGeom g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks, int* err) {
+  for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
+       i += i64(gridDim.x) * kBinBlock) {
+    i64 tile_lin = 0;
+    i64 mul = 1;
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      i64 i0;
+      double frac;
+      ok &= cell_of(g, d, double(x.p[d][i]), i0, frac);
+      if (!ok) i0 = 0;
+      tile_lin += (i0 / g.tile[d]) * mul;
+      mul *= g.ntiles[d];
+    }
+    if (!ok) {
+      atomicOr(err, 1);
+      tile_lin = 0;
+    }
+    ranks[i] = atomicAdd(&counts[tile_lin], 1u);
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kBinBlock)
+    bin_scatter_kernel(BinGeom g, CoordPtrs<T> x, i64 M, const u32* ranks, const u32* bin_start,
+                       u32* perm, u32* local, T* f0, T* f1, T* f2) {
+  for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
+       i += i64(gridDim.x) * kBinBlock) {
+    i64 tile_lin = 0;
+    i64 mul = 1;
+    int l[3] = {0, 0, 0};
+    double fr[3] = {0, 0, 0};
+    i64 i0[3] = {0, 0, 0};
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) ok &= cell_of(g, d, double(x.p[d][i]), i0[d], fr[d]);
+    // A non-finite point went to tile 0 in pass 1 (the host then rejects the point set); it
+    // must land in the same tile here so that its slot stays inside tile 0's range.
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      if (!ok) {
+        i0[d] = 0;
+        fr[d] = -0.5 * g.w;
+      }
+      const i64 t = i0[d] / g.tile[d];
+      l[d] = int(i0[d] - t * g.tile[d]);
+      tile_lin += t * mul;
+      mul *= g.ntiles[d];
+    }
+    const u32 pos = bin_start[tile_lin] + ranks[i];
+    perm[pos] = u32(i);
+    local[pos] = pack_local(DIM, l[0], l[1], l[2]);
+    f0[pos] = T(fr[0]);
+    if (DIM > 1) f1[pos] = T(fr[1]);
+    if (DIM > 2) f2[pos] = T(fr[2]);
+  }
+}
+
+// ---- exclusive scan ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kScanThreads * kScanItems;
+
+// Block-wide exclusive scan of one value per thread; returns the block total in *total.
+template <int THREADS>
+__device__ __forceinline__ u64 block_exclusive_scan(u64 v, u64* total) {
+  __shared__ u64 warp_sums[THREADS / 32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  u64 incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u64 n = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += n;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    u64 s = lane < THREADS / 32 ? warp_sums[lane] : 0;
+    u64 si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 n = __shfl_up_sync(0xffffffffu, si, o);
+      if (lane >= o) si += n;
+    }
+    if (lane < THREADS / 32) warp_sums[lane] = si - s;  // exclusive warp offsets
+    if (lane == THREADS / 32 - 1) *total = si;
+  }
+  __syncthreads();
+  const u64 res = warp_sums[warp] + incl - v;
+  __syncthreads();
+  return res;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_block_sums_kernel(const u32* in, i64 n, u32* block_sums) {
+  const i64 base = i64(blockIdx.x) * kScanChunk + threadIdx.x * kScanItems;
+  u64 s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) s += in[base + k];
+  }
+  __shared__ u64 total;
+  block_exclusive_scan<kScanThreads>(s, &total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = u32(total);
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_top_kernel(u32* block_sums, i64 nb) {
+  __shared__ u64 total;
+  u64 carry = 0;
+  for (i64 off = 0; off < nb; off += kScanChunk) {
+    const i64 base = off + threadIdx.x * kScanItems;
+    u32 v[kScanItems];
+    u64 s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      v[k] = (base + k < nb) ? block_sums[base + k] : 0u;
+      s += v[k];
+    }
+    u64 run = block_exclusive_scan<kScanThreads>(s, &total) + carry;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < nb) block_sums[base + k] = u32(run);
+      run += v[k];
+    }
+    __syncthreads();
+    carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) block_sums[nb] = u32(carry);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_apply_kernel(const u32* in, i64 n, const u32* block_offsets, i64 nb, u32* out) {
+  const i64 base = i64(blockIdx.x) * kScanChunk + threadIdx.x * kScanItems;
+  u32 v[kScanItems];
+  u64 s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0u;
+    s += v[k];
+  }
+  __shared__ u64 total;
+  u64 run = block_exclusive_scan<kScanThreads>(s, &total) + block_offsets[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = u32(run);
+    run += v[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = block_offsets[nb];
+}
+
+int grid_for(i64 n, int block) {
+  i64 g = (n + block - 1) / block;
+  const i64 cap = 148 * 32;  // grid-stride loops beyond this many blocks
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return int(g);
+}
+
+}  // namespace
+
+template <typename T>
+void launch_bin_count(const BinGeom& g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks,
+                      int* err_flag, cudaStream_t stream) {
+  if (M <= 0) return;
+  const int grid = grid_for(M, kBinBlock);
+  switch (g.dim) {
+    case 1: bin_count_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, counts, ranks, err_flag); break;
+    case 2: bin_count_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, counts, ranks, err_flag); break;
+    default: bin_count_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, counts, ranks, err_flag); break;
+  }
+  NNB_LAUNCH_CHECK();
+}
+
+i64 scan_tmp_words(i64 n) { return (n + kScanChunk - 1) / kScanChunk + 1; }
+
+void launch_exclusive_scan(const u32* counts, u32* out, i64 n, u32* tmp, cudaStream_t stream) {
+  const i64 nb = (n + kScanChunk - 1) / kScanChunk;
+  if (nb <= 0) return;
+  scan_block_sums_kernel<<<unsigned(nb), kScanThreads, 0, stream>>>(counts, n, tmp);
+  NNB_LAUNCH_CHECK();
+  scan_top_kernel<<<1, kScanThreads, 0, stream>>>(tmp, nb);
+  NNB_LAUNCH_CHECK();
+  scan_apply_kernel<<<unsigned(nb), kScanThreads, 0, stream>>>(counts, n, tmp, nb, out);
+  NNB_LAUNCH_CHECK();
+}
+
+template <typename T, typename TF>
+void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
+                        const u32* bin_start, u32* perm, u32* local, TF* f0, TF* f1, TF* f2,
+                        cudaStream_t stream) {
+  static_assert(std::is_same<T, TF>::value, "fractions are stored in the plan precision");
+  if (M <= 0) return;
+  const int grid = grid_for(M, kBinBlock);
+  switch (g.dim) {
+    case 1: bin_scatter_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
+    case 2: bin_scatter_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
+    default: bin_scatter_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
+  }
+  NNB_LAUNCH_CHECK();
+}
+
+template void launch_bin_count<float>(const BinGeom&, CoordPtrs<float>, i64, u32*, u32*, int*, cudaStream_t);
+template void launch_bin_count<double>(const BinGeom&, CoordPtrs<double>, i64, u32*, u32*, int*, cudaStream_t);
+template void launch_bin_scatter<float, float>(const BinGeom&, CoordPtrs<float>, i64, const u32*, const u32*, u32*, u32*, float*, float*, float*, cudaStream_t);
+template void launch_bin_scatter<double, double>(const BinGeom&, CoordPtrs<double>, i64, const u32*, const u32*, u32*, u32*, double*, double*, double*, cudaStream_t);
+
+}  // namespace nnb

@@ -1,0 +1,137 @@
+// Shared definitions of the B200 NUFFT engine: complex helpers, error handling, grid geometry.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "neonufft/enums.h"
+#include "neonufft/exceptions.hpp"
+
+namespace nnb {
+
+using i64 = std::int64_t;
+using u32 = std::uint32_t;
+using u64 = std::uint64_t;
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kTwoPiInv = 1.0 / (2.0 * kPi);
+
+// ---------------------------------------------------------------------------------------------
+// Complex storage types (interleaved re/im, identical layout to cuComplex / cuDoubleComplex).
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+template <typename T>
+using cplx_t = typename Cplx<T>::type;
+
+template <typename C>
+__host__ __device__ __forceinline__ C cmul(C a, C b) {
+  return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+
+// ---------------------------------------------------------------------------------------------
+// Error handling: host code throws the reference exception types; the C ABI translates them.
+// Messages are copied into a per-thread buffer so that the exception may keep a const char*.
+// ---------------------------------------------------------------------------------------------
+const char* store_message(const std::string& msg);
+
+[[noreturn]] void throw_gpu(cudaError_t err, const char* what, const char* file, int line);
+[[noreturn]] void throw_fft(cufftResult err, const char* what, const char* file, int line);
+[[noreturn]] void throw_input(const std::string& msg);
+[[noreturn]] void throw_internal(const std::string& msg);
+
+#define NNB_CUDA(expr)                                                        \
+  do {                                                                        \
+    cudaError_t nnb_err_ = (expr);                                            \
+    if (nnb_err_ != cudaSuccess) ::nnb::throw_gpu(nnb_err_, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+#define NNB_CUFFT(expr)                                                       \
+  do {                                                                        \
+    cufftResult nnb_err_ = (expr);                                            \
+    if (nnb_err_ != CUFFT_SUCCESS) ::nnb::throw_fft(nnb_err_, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+// Counts one engine kernel launch and checks the launch status of the last kernel.
+void count_launch();
+#define NNB_LAUNCH_CHECK()        \
+  do {                            \
+    ::nnb::count_launch();        \
+    NNB_CUDA(cudaGetLastError()); \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// Geometry of a binned point set on a fine grid.
+//
+// Points are rescaled to p = frac(((x - offset) * scale + pi) / 2pi) in [0, 1), placed at
+// loc = p * nf on the fine grid, and assigned to the subproblem tile containing their first
+// kernel cell i0 = ceil(loc - w/2) (wrapped periodically). This is the rescaling of the
+// reference (src/neonufft/gpu/kernels/rescale_loc_kernel.cu:107-121 and :167-179, affine part
+// for type 3), computed here in double precision for every plan precision.
+// ---------------------------------------------------------------------------------------------
+struct BinGeom {
+  int dim;
+  int w;              // kernel width (n_spread)
+  i64 nf[3];          // fine grid dims (1 for unused dims)
+  int tile[3];        // tile dims (1 for unused dims)
+  int ntiles[3];      // number of tiles per dim
+  i64 total_tiles;
+  double offset[3];   // affine pre-transform (type 3); 0 / 1 otherwise
+  double scale[3];
+};
+
+// Packed tile-local start cell of a point: 1D 32 bits; 2D 16+16; 3D 11+11+10 (x, y, z).
+__host__ __device__ __forceinline__ u32 pack_local(int dim, int lx, int ly, int lz) {
+  if (dim == 1) return u32(lx);
+  if (dim == 2) return u32(lx) | (u32(ly) << 16);
+  return u32(lx) | (u32(ly) << 11) | (u32(lz) << 22);
+}
+__host__ __device__ __forceinline__ void unpack_local(int dim, u32 v, int& lx, int& ly, int& lz) {
+  if (dim == 1) {
+    lx = int(v); ly = 0; lz = 0;
+  } else if (dim == 2) {
+    lx = int(v & 0xFFFFu); ly = int(v >> 16); lz = 0;
+  } else {
+    lx = int(v & 0x7FFu); ly = int((v >> 11) & 0x7FFu); lz = int(v >> 22);
+  }
+}
+constexpr int kMaxTileBits3[3] = {11, 11, 10};
+
+// Device-side view of a bin-sorted point set (structure of arrays, length M, sorted by tile).
+template <typename T>
+struct SortedPoints {
+  const u32* perm;       // original point index
+  const u32* local;      // packed tile-local start cell
+  const T* frac[3];      // kernel argument of the first cell, i0 - loc, in [-w/2, -w/2 + 1]
+  const u32* bin_start;  // total_tiles + 1 offsets into the sorted arrays
+};
+
+// ES kernel (exponential of semicircle): phi(x) = exp(beta * (sqrt(1 - c x^2) - 1)) for
+// |x| < w/2, else 0, c = 4 / w^2 (reference src/neonufft/gpu/kernels/es_kernel_eval.cuh:18-44).
+template <typename T>
+__device__ __forceinline__ T es_eval(T x, T beta, T c);
+
+template <>
+__device__ __forceinline__ float es_eval<float>(float x, float beta, float c) {
+  const float arg = 1.f - c * x * x;
+  return arg > 0.f ? expf(beta * (sqrtf(arg) - 1.f)) : 0.f;
+}
+template <>
+__device__ __forceinline__ double es_eval<double>(double x, double beta, double c) {
+  const double arg = 1.0 - c * x * x;
+  return arg > 0.0 ? exp(beta * (sqrt(arg) - 1.0)) : 0.0;
+}
+
+}  // namespace nnb

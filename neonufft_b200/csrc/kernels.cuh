@@ -1,0 +1,110 @@
+// Launchers of the engine's device kernels. Every launcher enqueues on `stream` and checks the
+// launch status; none synchronises.
+#pragma once
+
+#include "common.cuh"
+
+namespace nnb {
+
+template <typename T>
+struct CoordPtrs {
+  const T* p[3];
+};
+
+// ---- binning (binning.cu) -------------------------------------------------------------------
+// Pass 1: per point, tile index and rank within the tile (one int atomic per point).
+template <typename T>
+void launch_bin_count(const BinGeom& g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks,
+                      int* err_flag, cudaStream_t stream);
+// Exclusive scan of n counts into out[0..n] (out[n] = total). tmp needs scan_tmp_words(n).
+i64 scan_tmp_words(i64 n);
+void launch_exclusive_scan(const u32* counts, u32* out, i64 n, u32* tmp, cudaStream_t stream);
+// Pass 2: permutation and packed per-point data in tile order.
+template <typename T, typename TF>
+void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
+                        const u32* bin_start, u32* perm, u32* local, TF* frac0, TF* frac1,
+                        TF* frac2, cudaStream_t stream);
+
+// ---- spreading (spread.cu) ------------------------------------------------------------------
+template <typename T>
+struct SpreadArgs {
+  BinGeom g;
+  SortedPoints<T> pts;
+  const cplx_t<T>* in;        // strengths, original point order (batch b at in + b * in_bdist)
+  const cplx_t<T>* prephase;  // optional per-point factor, original order
+  cplx_t<T>* grid;            // fine grid (batch b at grid + b * grid_bdist), accumulated into
+  i64 in_bdist;
+  i64 grid_bdist;
+  int batch;
+  T beta;
+  T c;
+};
+template <typename T>
+void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream);
+
+// ---- interpolation (interp.cu) --------------------------------------------------------------
+template <typename T>
+struct InterpArgs {
+  BinGeom g;
+  SortedPoints<T> pts;
+  const cplx_t<T>* grid;       // fine grid
+  const cplx_t<T>* postphase;  // optional per-point factor, original order
+  cplx_t<T>* out;              // original point order
+  T beta;
+  T c;
+};
+template <typename T>
+void launch_interp(const InterpArgs<T>& a, cudaStream_t stream);
+
+// ---- deconvolution (deconv.cu) --------------------------------------------------------------
+template <typename T>
+struct DeconvArgs {
+  int dim;
+  int order;        // NeonufftModeOrder
+  i64 nf[3];        // fine grid
+  i64 modes[3];     // mode box
+  i64 stride[3];    // strides (elements) of the user mode array
+  const T* corr[3]; // 1 / phi_hat per dim, nf/2 + 1 values
+};
+// Type 1: out(modes, strided) = fine(k mod nf) * prod corr.
+template <typename T>
+void launch_downsample(const DeconvArgs<T>& a, const cplx_t<T>* fine, cplx_t<T>* out,
+                       cudaStream_t stream);
+// Type 2 / type 3 stage 2: fine = zero-padded modes * prod corr (writes every fine cell).
+template <typename T>
+void launch_upsample(const DeconvArgs<T>& a, const cplx_t<T>* in, cplx_t<T>* fine,
+                     cudaStream_t stream);
+
+// ---- type 3 (t3.cu) -------------------------------------------------------------------------
+// min / max of each coordinate array into out[2d] (min), out[2d+1] (max), as double.
+template <typename T>
+void launch_min_max(int dim, CoordPtrs<T> x, i64 M, unsigned long long* enc_out,
+                    cudaStream_t stream);
+void decode_min_max(const unsigned long long* enc, int n, double* out);
+void init_min_max(unsigned long long* enc_host, int n);
+
+template <typename T>
+void launch_prephase(int dim, int sign, CoordPtrs<T> x, i64 M, const double* out_offset,
+                     cplx_t<T>* pre, cudaStream_t stream);
+
+struct PostphaseQuad {
+  int n;
+  double z[32];
+  double kv[32];
+};
+template <typename T>
+void launch_postphase(int dim, int sign, CoordPtrs<T> s, i64 K, const double* out_offset,
+                      const double* in_offset, const double* scale, const PostphaseQuad& q,
+                      cplx_t<T>* post, cudaStream_t stream);
+
+// ---- FP64 direct sums (direct.cu) ------------------------------------------------------------
+void launch_direct_type1(int dim, int sign, i64 M, const double* const* loc, const double* in,
+                         i64 S, const i64* modes_idx, double* out, cudaStream_t stream);
+void launch_direct_type2(int dim, int sign, const i64* n_modes, const double* in,
+                         const double* const* loc, i64 S, const i64* point_idx, double* out,
+                         cudaStream_t stream);
+void launch_direct_type3(int dim, int sign, i64 M, const double* const* in_loc, const double* in,
+                         const double* const* out_loc, i64 S, const i64* target_idx,
+                         double* out, cudaStream_t stream);
+
+}  // namespace nnb

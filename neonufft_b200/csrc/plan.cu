@@ -1,0 +1,565 @@
+// Plan implementations (see plan.hpp).
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace nnb {
+
+namespace {
+
+template <typename T>
+constexpr bool is_single() {
+  return std::is_same<T, float>::value;
+}
+
+template <typename T>
+void upload(DevArray<T>& dst, const std::vector<double>& src, cudaStream_t stream) {
+  std::vector<T> host(src.begin(), src.end());
+  dst.reserve(host.size());
+  NNB_CUDA(cudaMemcpyAsync(dst.data(), host.data(), sizeof(T) * host.size(),
+                           cudaMemcpyHostToDevice, stream));
+  // pageable source: the copy has been staged when cudaMemcpyAsync returns, but keep the
+  // host vector alive until the stream reaches it to stay independent of that detail.
+  NNB_CUDA(cudaStreamSynchronize(stream));
+}
+
+template <typename T>
+CoordPtrs<T> coords(int dim, const void* const* loc) {
+  CoordPtrs<T> c{{nullptr, nullptr, nullptr}};
+  if (!loc) return c;
+  for (int d = 0; d < dim; ++d) c.p[d] = static_cast<const T*>(loc[d]);
+  return c;
+}
+
+void check_strides(int dim, const i64* modes, const i64* strides) {
+  if (!strides) throw_input("null strides");
+  for (int d = 0; d < dim; ++d) {
+    if (strides[d] < 1 && modes[d] > 1) throw_input("strides must be positive");
+  }
+}
+
+}  // namespace
+
+void validate_options(const NnbOptions& opt) {
+  if (!(opt.tol > 0.0) || !std::isfinite(opt.tol)) throw_input("tol must be positive and finite");
+  if (!(opt.upsampfac > 1.0) || !std::isfinite(opt.upsampfac)) {
+    throw_input("upsampfac must be greater than 1");
+  }
+  if (opt.order != NEONUFFT_MODE_ORDER_FFT && opt.order != NEONUFFT_MODE_ORDER_CMCL) {
+    throw_input("invalid mode order");
+  }
+  if (opt.kernel_type != NEONUFFT_ES_KERNEL) throw_input("invalid kernel type");
+  if (!std::isfinite(opt.recenter_threshold)) throw_input("invalid recenter threshold");
+  for (int d = 0; d < 3; ++d) {
+    if (opt.tile[d] < 0) throw_input("invalid tile shape");
+  }
+}
+
+// =============================================================================================
+// Type 1 / type 2.
+// =============================================================================================
+template <typename T>
+class PlanImpl final : public PlanBase {
+public:
+  PlanImpl(int dim, const NnbOptions& opt, int sign, i64 M, const void* const* loc,
+           const i64* modes, cudaStream_t stream, const NnbAllocator* alloc)
+      : alloc_(std::make_shared<DeviceAllocator>(alloc)),
+        dim_(dim),
+        opt_(opt),
+        sign_(sign < 0 ? -1 : 1),
+        stream_(stream),
+        points_(alloc_) {
+    if (!modes) throw_input("null modes");
+    for (int d = 0; d < 3; ++d) {
+      modes_[d] = 1;
+      nf_[d] = 1;
+    }
+    for (int d = 0; d < dim; ++d) {
+      if (modes[d] < 1) throw_input("number of modes must be positive");
+      modes_[d] = modes[d];
+    }
+    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+    if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
+    for (int d = 0; d < dim; ++d) nf_[d] = fine_grid_size(modes_[d], opt.upsampfac, kp_.w);
+    fft_ = std::make_unique<FftGrid<T>>(alloc_, dim, nf_, sign_, stream_);
+    for (int d = 0; d < dim; ++d) {
+      corr_[d].set_allocator(alloc_);
+      upload(corr_[d], deconv_factors(kp_, nf_[d]), stream_);
+    }
+    choose_tile(dim, kp_.w, sizeof(cplx_t<T>), nf_, opt.tile, tile_);
+    geom_ = make_geom(dim, kp_.w, nf_, tile_, nullptr, nullptr);
+    set_points(M, loc);
+  }
+
+  void set_points(i64 M, const void* const* loc) override {
+    if (M < 0) throw_input("negative number of points");
+    if (M > 0 && !loc) throw_input("null coordinate pointers");
+    ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
+    points_.build(geom_, coords<T>(dim_, loc), M, stream_);
+  }
+
+  void transform_type_1(const void* in, void* out, const i64* out_strides) override {
+    const i64 M = points_.size();
+    if (!out) throw_input("null output");
+    if (M > 0 && !in) throw_input("null input");
+    check_strides(dim_, modes_, out_strides);
+    NNB_CUDA(cudaMemsetAsync(fft_->data(), 0, sizeof(cplx_t<T>) * fft_->cells(), stream_));
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_SPREAD);
+      if (M > 0) {
+        SpreadArgs<T> a{};
+        a.g = geom_;
+        a.pts = points_.view();
+        a.in = static_cast<const cplx_t<T>*>(in);
+        a.prephase = nullptr;
+        a.grid = fft_->data();
+        a.in_bdist = 0;
+        a.grid_bdist = 0;
+        a.batch = 1;
+        a.beta = T(kp_.beta);
+        a.c = T(kp_.c);
+        launch_spread<T>(a, stream_);
+      }
+    }
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
+      fft_->exec(stream_);
+    }
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
+      launch_downsample<T>(deconv_args(out_strides), fft_->data(), static_cast<cplx_t<T>*>(out),
+                           stream_);
+    }
+  }
+
+  void transform_type_2(const void* in, const i64* in_strides, void* out) override {
+    const i64 M = points_.size();
+    if (!in) throw_input("null input");
+    if (M > 0 && !out) throw_input("null output");
+    check_strides(dim_, modes_, in_strides);
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
+      launch_upsample<T>(deconv_args(in_strides), static_cast<const cplx_t<T>*>(in),
+                         fft_->data(), stream_);
+    }
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
+      fft_->exec(stream_);
+    }
+    if (M > 0) {
+      ScopedStage st(timer_, stream_, NNB_STAGE_INTERP);
+      InterpArgs<T> a{};
+      a.g = geom_;
+      a.pts = points_.view();
+      a.grid = fft_->data();
+      a.postphase = nullptr;
+      a.out = static_cast<cplx_t<T>*>(out);
+      a.beta = T(kp_.beta);
+      a.c = T(kp_.c);
+      launch_interp<T>(a, stream_);
+    }
+  }
+
+  void info(NnbPlanInfo* info) const override {
+    *info = NnbPlanInfo{};
+    info->dim = dim_;
+    info->precision = is_single<T>() ? NNB_FLOAT : NNB_DOUBLE;
+    info->n_spread = kp_.w;
+    info->spread_method = 1;
+    info->es_beta = kp_.beta;
+    for (int d = 0; d < 3; ++d) {
+      info->grid[d] = nf_[d];
+      info->spread_grid[d] = nf_[d];
+      info->tile[d] = d < dim_ ? tile_[d] : 1;
+    }
+    info->num_in = points_.size();
+    info->num_out = 0;
+    info->batch_size = 1;
+    info->device_bytes = alloc_->in_use();
+  }
+
+  StageTimer& timer() override { return timer_; }
+  cudaStream_t stream() const override { return stream_; }
+
+private:
+  DeconvArgs<T> deconv_args(const i64* strides) const {
+    DeconvArgs<T> a{};
+    a.dim = dim_;
+    a.order = opt_.order;
+    for (int d = 0; d < 3; ++d) {
+      a.nf[d] = nf_[d];
+      a.modes[d] = modes_[d];
+      a.stride[d] = d < dim_ ? strides[d] : 0;
+      a.corr[d] = d < dim_ ? corr_[d].data() : nullptr;
+    }
+    return a;
+  }
+
+  std::shared_ptr<DeviceAllocator> alloc_;
+  int dim_;
+  NnbOptions opt_;
+  int sign_;
+  cudaStream_t stream_;
+  KernelParam kp_;
+  i64 modes_[3];
+  i64 nf_[3];
+  int tile_[3] = {1, 1, 1};
+  BinGeom geom_{};
+  std::unique_ptr<FftGrid<T>> fft_;
+  DevArray<T> corr_[3];
+  PointSet<T> points_;
+  StageTimer timer_;
+};
+
+// =============================================================================================
+// Type 3.
+// =============================================================================================
+template <typename T>
+class PlanT3Impl final : public PlanT3Base {
+public:
+  PlanT3Impl(int dim, const NnbOptions& opt, int sign, i64 batch, cudaStream_t stream,
+             const NnbAllocator* alloc)
+      : alloc_(std::make_shared<DeviceAllocator>(alloc)),
+        dim_(dim),
+        opt_(opt),
+        sign_(sign < 0 ? -1 : 1),
+        batch_(batch),
+        stream_(stream),
+        spread_grid_(alloc_),
+        prephase_(alloc_),
+        postphase_(alloc_),
+        in_points_(alloc_),
+        out_points_(alloc_) {
+    if (batch < 1) throw_input("batch size must be positive");
+    if (batch > 65535) throw_input("batch size above 65535");
+    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+    if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
+    for (auto& c : corr_) c.set_allocator(alloc_);
+  }
+
+  // Bounds from the point sets, computed on the device (reference
+  // src/neonufft/gpu/plan_t3_impl.hpp:88-111), then the bounds constructor path.
+  void init_from_points(i64 M, const void* const* in_pts, i64 K, const void* const* out_pts) {
+    if (M < 0 || K < 0) throw_input("negative number of points");
+    if ((M > 0 && !in_pts) || (K > 0 && !out_pts)) throw_input("null coordinate pointers");
+    double in_min[3] = {0, 0, 0}, in_max[3] = {0, 0, 0};
+    double out_min[3] = {0, 0, 0}, out_max[3] = {0, 0, 0};
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_PHASE);
+      DevArray<unsigned long long> enc(alloc_);
+      enc.reserve(4 * dim_);
+      unsigned long long host[12];
+      init_min_max(host, 4 * dim_);
+      NNB_CUDA(cudaMemcpyAsync(enc.data(), host, sizeof(host[0]) * 4 * dim_,
+                               cudaMemcpyHostToDevice, stream_));
+      if (M > 0) launch_min_max<T>(dim_, coords<T>(dim_, in_pts), M, enc.data(), stream_);
+      if (K > 0) {
+        launch_min_max<T>(dim_, coords<T>(dim_, out_pts), K, enc.data() + 2 * dim_, stream_);
+      }
+      NNB_CUDA(cudaMemcpyAsync(host, enc.data(), sizeof(host[0]) * 4 * dim_,
+                               cudaMemcpyDeviceToHost, stream_));
+      NNB_CUDA(cudaStreamSynchronize(stream_));
+      double mm[12];
+      decode_min_max(host, 4 * dim_, mm);
+      for (int d = 0; d < dim_; ++d) {
+        if (M > 0) {
+          in_min[d] = mm[2 * d];
+          in_max[d] = mm[2 * d + 1];
+        }
+        if (K > 0) {
+          out_min[d] = mm[2 * dim_ + 2 * d];
+          out_max[d] = mm[2 * dim_ + 2 * d + 1];
+        }
+      }
+    }
+    init(in_min, in_max, out_min, out_max);
+    set_input_points(M, in_pts);
+    set_output_points(K, out_pts);
+  }
+
+  // Geometry, grids, FFT plan and correction factors (reference plan_t3_impl.hpp:255-306).
+  void init(const double* in_min, const double* in_max, const double* out_min,
+            const double* out_max) {
+    for (int d = 0; d < dim_; ++d) {
+      if (!(T(in_min[d]) <= T(in_max[d]))) throw_input("Invalid input bounds.");
+      if (!(T(out_min[d]) <= T(out_max[d]))) throw_input("Invalid output bounds.");
+    }
+    i64 spread_cells = 1;
+    for (int d = 0; d < 3; ++d) {
+      nf1_[d] = 1;
+      nfft_[d] = 1;
+      C_[d] = D_[d] = 0;
+      gamma_[d] = h_[d] = 1;
+    }
+    for (int d = 0; d < dim_; ++d) {
+      const T3Dim<T> g = t3_geometry<T>(kp_.w, opt_.upsampfac, T(opt_.recenter_threshold),
+                                        T(in_min[d]), T(in_max[d]), T(out_min[d]),
+                                        T(out_max[d]));
+      nf1_[d] = g.spread_grid;
+      nfft_[d] = g.fft_grid;
+      C_[d] = double(g.input_offset);
+      D_[d] = double(g.output_offset);
+      gamma_[d] = double(g.gamma);
+      h_[d] = double(g.h);
+      spread_cells *= nf1_[d];
+    }
+    spread_cells_ = spread_cells;
+    spread_grid_.reserve(size_t(spread_cells * batch_));
+    NNB_CUDA(cudaMemsetAsync(spread_grid_.data(), 0,
+                             sizeof(cplx_t<T>) * size_t(spread_cells * batch_), stream_));
+    fft_ = std::make_unique<FftGrid<T>>(alloc_, dim_, nfft_, sign_, stream_);
+    for (int d = 0; d < dim_; ++d) upload(corr_[d], deconv_factors(kp_, nfft_[d]), stream_);
+    const PhiHatQuad quad = phi_hat_quadrature(kp_);
+    if (quad.z.size() > 32) throw_internal("too many quadrature nodes");
+    quad_.n = int(quad.z.size());
+    for (int i = 0; i < quad_.n; ++i) {
+      quad_.z[i] = quad.z[i];
+      quad_.kv[i] = quad.kv[i];
+    }
+    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nf1_, opt_.tile, in_tile_);
+    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nfft_, opt_.tile, out_tile_);
+    NNB_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  void set_input_points(i64 M, const void* const* pts) override {
+    if (M < 0) throw_input("negative number of points");
+    if (M > 0 && !pts) throw_input("null coordinate pointers");
+    const CoordPtrs<T> x = coords<T>(dim_, pts);
+    bool need_pre = false;
+    for (int d = 0; d < dim_; ++d) need_pre |= (D_[d] != 0.0);
+    if (need_pre && M > 0) {
+      ScopedStage st(timer_, stream_, NNB_STAGE_PHASE);
+      prephase_.reserve(size_t(M));
+      launch_prephase<T>(dim_, sign_, x, M, D_, prephase_.data(), stream_);
+      has_prephase_ = true;
+    } else {
+      prephase_.release();
+      has_prephase_ = false;
+    }
+    double scale[3];
+    for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? 1.0 / gamma_[d] : 1.0;
+    const BinGeom g = make_geom(dim_, kp_.w, nf1_, in_tile_, C_, scale);
+    ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
+    in_points_.build(g, x, M, stream_);
+  }
+
+  void set_output_points(i64 K, const void* const* pts) override {
+    if (K < 0) throw_input("negative number of points");
+    if (K > 0 && !pts) throw_input("null coordinate pointers");
+    const CoordPtrs<T> s = coords<T>(dim_, pts);
+    double scale[3];
+    for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? gamma_[d] * h_[d] : 1.0;
+    const BinGeom g = make_geom(dim_, kp_.w, nfft_, out_tile_, D_, scale);
+    {
+      ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
+      out_points_.build(g, s, K, stream_);
+    }
+    ScopedStage st(timer_, stream_, NNB_STAGE_PHASE);
+    postphase_.reserve(size_t(K));
+    if (K > 0) {
+      launch_postphase<T>(dim_, sign_, s, K, D_, C_, scale, quad_, postphase_.data(), stream_);
+    }
+    NNB_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  void add_input(const void* in, i64 bdist) override {
+    const i64 M = in_points_.size();
+    if (M == 0) return;
+    if (!in) throw_input("null input");
+    if (bdist <= 0) bdist = M;
+    ScopedStage st(timer_, stream_, NNB_STAGE_SPREAD);
+    SpreadArgs<T> a{};
+    a.g = in_points_.geom();
+    a.pts = in_points_.view();
+    a.in = static_cast<const cplx_t<T>*>(in);
+    a.prephase = has_prephase_ ? prephase_.data() : nullptr;
+    a.grid = spread_grid_.data();
+    a.in_bdist = bdist;
+    a.grid_bdist = spread_cells_;
+    a.batch = int(batch_);
+    a.beta = T(kp_.beta);
+    a.c = T(kp_.c);
+    launch_spread<T>(a, stream_);
+  }
+
+  void transform(void* out, i64 bdist) override {
+    const i64 K = out_points_.size();
+    if (K == 0) return;
+    if (!out) throw_input("null output");
+    if (bdist <= 0) bdist = K;
+    DeconvArgs<T> dc{};
+    dc.dim = dim_;
+    dc.order = NEONUFFT_MODE_ORDER_CMCL;
+    i64 stride = 1;
+    for (int d = 0; d < 3; ++d) {
+      dc.nf[d] = nfft_[d];
+      dc.modes[d] = nf1_[d];
+      dc.stride[d] = stride;
+      stride *= nf1_[d];
+      dc.corr[d] = d < dim_ ? corr_[d].data() : nullptr;
+    }
+    for (i64 b = 0; b < batch_; ++b) {
+      {
+        ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
+        launch_upsample<T>(dc, spread_grid_.data() + b * spread_cells_, fft_->data(), stream_);
+      }
+      {
+        ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
+        fft_->exec(stream_);
+      }
+      ScopedStage st(timer_, stream_, NNB_STAGE_INTERP);
+      InterpArgs<T> a{};
+      a.g = out_points_.geom();
+      a.pts = out_points_.view();
+      a.grid = fft_->data();
+      a.postphase = postphase_.data();
+      a.out = static_cast<cplx_t<T>*>(out) + b * bdist;
+      a.beta = T(kp_.beta);
+      a.c = T(kp_.c);
+      launch_interp<T>(a, stream_);
+    }
+  }
+
+  void reset() override {
+    NNB_CUDA(cudaMemsetAsync(spread_grid_.data(), 0,
+                             sizeof(cplx_t<T>) * size_t(spread_cells_ * batch_), stream_));
+  }
+
+  void info(NnbPlanInfo* info) const override {
+    *info = NnbPlanInfo{};
+    info->dim = dim_;
+    info->precision = is_single<T>() ? NNB_FLOAT : NNB_DOUBLE;
+    info->n_spread = kp_.w;
+    info->spread_method = 1;
+    info->es_beta = kp_.beta;
+    for (int d = 0; d < 3; ++d) {
+      info->grid[d] = nfft_[d];
+      info->spread_grid[d] = nf1_[d];
+      info->tile[d] = d < dim_ ? in_tile_[d] : 1;
+      info->input_offset[d] = C_[d];
+      info->output_offset[d] = D_[d];
+      info->gamma[d] = gamma_[d];
+      info->h[d] = h_[d];
+    }
+    info->num_in = in_points_.size();
+    info->num_out = out_points_.size();
+    info->batch_size = batch_;
+    info->device_bytes = alloc_->in_use();
+  }
+
+  StageTimer& timer() override { return timer_; }
+  cudaStream_t stream() const override { return stream_; }
+
+private:
+  std::shared_ptr<DeviceAllocator> alloc_;
+  int dim_;
+  NnbOptions opt_;
+  int sign_;
+  i64 batch_;
+  cudaStream_t stream_;
+  KernelParam kp_;
+  i64 nf1_[3] = {1, 1, 1};
+  i64 nfft_[3] = {1, 1, 1};
+  double C_[3] = {0, 0, 0}, D_[3] = {0, 0, 0};
+  double gamma_[3] = {1, 1, 1}, h_[3] = {1, 1, 1};
+  int in_tile_[3] = {1, 1, 1};
+  int out_tile_[3] = {1, 1, 1};
+  i64 spread_cells_ = 0;
+  DevArray<cplx_t<T>> spread_grid_;
+  std::unique_ptr<FftGrid<T>> fft_;
+  DevArray<T> corr_[3];
+  PostphaseQuad quad_{};
+  DevArray<cplx_t<T>> prephase_;
+  DevArray<cplx_t<T>> postphase_;
+  bool has_prephase_ = false;
+  PointSet<T> in_points_;
+  PointSet<T> out_points_;
+  StageTimer timer_;
+};
+
+// =============================================================================================
+// Factories.
+// =============================================================================================
+namespace {
+void check_dim_prec(NnbPrecision prec, int dim) {
+  if (dim < 1 || dim > 3) throw_input("dimension must be 1, 2 or 3");
+  if (prec != NNB_FLOAT && prec != NNB_DOUBLE) throw_input("invalid precision");
+}
+}  // namespace
+
+std::unique_ptr<PlanBase> make_plan(NnbPrecision prec, int dim, const NnbOptions& opt, int sign,
+                                    i64 M, const void* const* loc, const i64* modes,
+                                    cudaStream_t stream, const NnbAllocator* alloc) {
+  check_dim_prec(prec, dim);
+  validate_options(opt);
+  if (prec == NNB_FLOAT) {
+    return std::make_unique<PlanImpl<float>>(dim, opt, sign, M, loc, modes, stream, alloc);
+  }
+  return std::make_unique<PlanImpl<double>>(dim, opt, sign, M, loc, modes, stream, alloc);
+}
+
+std::unique_ptr<PlanT3Base> make_plan_t3(NnbPrecision prec, int dim, const NnbOptions& opt,
+                                         int sign, i64 M, const void* const* in_pts, i64 K,
+                                         const void* const* out_pts, cudaStream_t stream,
+                                         i64 batch, const NnbAllocator* alloc) {
+  check_dim_prec(prec, dim);
+  validate_options(opt);
+  if (prec == NNB_FLOAT) {
+    auto p = std::make_unique<PlanT3Impl<float>>(dim, opt, sign, batch, stream, alloc);
+    p->init_from_points(M, in_pts, K, out_pts);
+    return p;
+  }
+  auto p = std::make_unique<PlanT3Impl<double>>(dim, opt, sign, batch, stream, alloc);
+  p->init_from_points(M, in_pts, K, out_pts);
+  return p;
+}
+
+std::unique_ptr<PlanT3Base> make_plan_t3_bounds(NnbPrecision prec, int dim,
+                                                const NnbOptions& opt, int sign,
+                                                const double* in_min, const double* in_max,
+                                                const double* out_min, const double* out_max,
+                                                cudaStream_t stream, i64 batch,
+                                                const NnbAllocator* alloc) {
+  check_dim_prec(prec, dim);
+  validate_options(opt);
+  if (!in_min || !in_max || !out_min || !out_max) throw_input("null bounds");
+  if (prec == NNB_FLOAT) {
+    auto p = std::make_unique<PlanT3Impl<float>>(dim, opt, sign, batch, stream, alloc);
+    p->init(in_min, in_max, out_min, out_max);
+    return p;
+  }
+  auto p = std::make_unique<PlanT3Impl<double>>(dim, opt, sign, batch, stream, alloc);
+  p->init(in_min, in_max, out_min, out_max);
+  return p;
+}
+
+namespace {
+template <typename T>
+u64 t3_grid_bytes(int dim, const NnbOptions& opt, const double* in_min, const double* in_max,
+                  const double* out_min, const double* out_max) {
+  const KernelParam kp = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+  u64 spread = 1, fft = 1;
+  for (int d = 0; d < dim; ++d) {
+    const T3Dim<T> g = t3_geometry<T>(kp.w, opt.upsampfac, T(opt.recenter_threshold),
+                                      T(in_min[d]), T(in_max[d]), T(out_min[d]), T(out_max[d]));
+    spread *= u64(g.spread_grid);
+    fft *= u64(g.fft_grid);
+  }
+  // Same accounting as the reference GPU plan (src/neonufft/gpu/plan_t3_impl.hpp:69-71):
+  // the FFT grid counts twice for the cuFFT work area.
+  return sizeof(cplx_t<T>) * (spread + 2 * fft);
+}
+}  // namespace
+
+u64 t3_grid_memory_size(NnbPrecision prec, int dim, const NnbOptions& opt, const double* in_min,
+                        const double* in_max, const double* out_min, const double* out_max) {
+  check_dim_prec(prec, dim);
+  validate_options(opt);
+  if (!in_min || !in_max || !out_min || !out_max) throw_input("null bounds");
+  if (prec == NNB_FLOAT) return t3_grid_bytes<float>(dim, opt, in_min, in_max, out_min, out_max);
+  return t3_grid_bytes<double>(dim, opt, in_min, in_max, out_min, out_max);
+}
+
+}  // namespace nnb

@@ -1,0 +1,326 @@
+// Host runtime: errors, allocator adapter, stage timer, cuFFT grid, point sets, tile choice.
+#include <cstring>
+#include <string>
+
+#include "runtime.hpp"
+
+namespace nnb {
+
+std::atomic<i64> g_kernel_launches{0};
+
+void count_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---- errors -----------------------------------------------------------------------------------
+namespace {
+thread_local std::string t_message;
+}
+
+const char* store_message(const std::string& msg) {
+  t_message = msg;
+  return t_message.c_str();
+}
+
+void throw_gpu(cudaError_t err, const char* what, const char* file, int line) {
+  std::string m = std::string("Neonufft:: GPU error: ") + cudaGetErrorString(err) + " (" + what +
+                  " at " + file + ":" + std::to_string(line) + ")";
+  if (err == cudaErrorMemoryAllocation) throw neonufft::MemoryAllocError(store_message(m));
+  throw neonufft::GPUError(store_message(m));
+}
+
+void throw_fft(cufftResult err, const char* what, const char* file, int line) {
+  std::string m = std::string("Neonufft:: cuFFT error ") + std::to_string(int(err)) + " (" +
+                  what + " at " + file + ":" + std::to_string(line) + ")";
+  if (err == CUFFT_ALLOC_FAILED) throw neonufft::MemoryAllocError(store_message(m));
+  throw neonufft::GPUFFTError(store_message(m));
+}
+
+void throw_input(const std::string& msg) {
+  throw neonufft::InputError(store_message("Neonufft:: Input error: " + msg));
+}
+
+void throw_internal(const std::string& msg) {
+  throw neonufft::InternalError(store_message("Neonufft:: Internal error: " + msg));
+}
+
+// ---- allocator ----------------------------------------------------------------------------------
+DeviceAllocator::DeviceAllocator(const NnbAllocator* a) {
+  if (a && a->allocate && a->deallocate) {
+    a_ = *a;
+    custom_ = true;
+  }
+}
+
+void* DeviceAllocator::allocate(size_t bytes) {
+  if (bytes == 0) return nullptr;
+  void* p = nullptr;
+  if (custom_) {
+    p = a_.allocate(a_.ctx, bytes);
+  } else {
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+    }
+  }
+  if (!p) {
+    throw neonufft::MemoryAllocError(store_message(
+        "Neonufft:: Memory allocation error: device allocation of " + std::to_string(bytes) +
+        " bytes failed"));
+  }
+  in_use_ += bytes;
+  return p;
+}
+
+void DeviceAllocator::deallocate(void* p, size_t bytes) noexcept {
+  if (!p) return;
+  in_use_ -= bytes;
+  if (custom_) {
+    a_.deallocate(a_.ctx, p);
+  } else {
+    (void)cudaFree(p);
+  }
+}
+
+// ---- stage timer ------------------------------------------------------------------------------
+StageTimer::~StageTimer() {
+  for (auto& p : pending_) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (auto e : pool_) cudaEventDestroy(e);
+  if (open_event_) cudaEventDestroy(open_event_);
+}
+
+cudaEvent_t StageTimer::get_event() {
+  if (!pool_.empty()) {
+    cudaEvent_t e = pool_.back();
+    pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  NNB_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+void StageTimer::begin(cudaStream_t s, int stage) {
+  if (!enabled_) return;
+  open_event_ = get_event();
+  open_stage_ = stage;
+  NNB_CUDA(cudaEventRecord(open_event_, s));
+}
+
+void StageTimer::end(cudaStream_t s, int stage) {
+  if (!enabled_ || open_stage_ != stage || !open_event_) return;
+  cudaEvent_t b = get_event();
+  if (cudaEventRecord(b, s) != cudaSuccess) {
+    pool_.push_back(b);
+    return;
+  }
+  pending_.push_back(Pending{stage, open_event_, b});
+  open_event_ = nullptr;
+  open_stage_ = -1;
+}
+
+void StageTimer::collect(cudaStream_t s, double* ms, i64* count, bool reset) {
+  NNB_CUDA(cudaStreamSynchronize(s));
+  for (auto& p : pending_) {
+    float t = 0.f;
+    NNB_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+    ms_[p.stage] += t;
+    count_[p.stage] += 1;
+    pool_.push_back(p.a);
+    pool_.push_back(p.b);
+  }
+  pending_.clear();
+  for (int i = 0; i < NNB_STAGE_COUNT; ++i) {
+    if (ms) ms[i] = ms_[i];
+    if (count) count[i] = count_[i];
+  }
+  if (reset) {
+    for (int i = 0; i < NNB_STAGE_COUNT; ++i) {
+      ms_[i] = 0;
+      count_[i] = 0;
+    }
+  }
+}
+
+// ---- cuFFT grid -------------------------------------------------------------------------------
+template <typename T>
+FftGrid<T>::FftGrid(std::shared_ptr<DeviceAllocator> alloc, int dim, const i64* nf, int sign,
+                    cudaStream_t stream)
+    : grid_(alloc), work_(alloc), dim_(dim), sign_(sign) {
+  for (int d = 0; d < dim; ++d) {
+    nf_[d] = nf[d];
+    cells_ *= nf[d];
+  }
+  grid_.reserve(size_t(cells_));
+  // cuFFT is row-major; the grid is column-major (x fastest), so dims are passed reversed.
+  int n[3];
+  for (int d = 0; d < dim; ++d) {
+    if (nf[d] > i64(0x7fffffff)) throw_input("fine grid dimension too large for cuFFT");
+    n[dim - 1 - d] = int(nf[d]);
+  }
+  NNB_CUFFT(cufftCreate(&plan_));
+  has_plan_ = true;
+  NNB_CUFFT(cufftSetAutoAllocation(plan_, 0));
+  size_t ws = 0;
+  const cufftType type = std::is_same<T, float>::value ? CUFFT_C2C : CUFFT_Z2Z;
+  NNB_CUFFT(cufftMakePlanMany(plan_, dim, n, nullptr, 1, 0, nullptr, 1, 0, type, 1, &ws));
+  work_.reserve(ws);
+  NNB_CUFFT(cufftSetWorkArea(plan_, work_.data()));
+  NNB_CUFFT(cufftSetStream(plan_, stream));
+}
+
+template <typename T>
+FftGrid<T>::~FftGrid() {
+  if (has_plan_) cufftDestroy(plan_);
+}
+
+template <typename T>
+void FftGrid<T>::exec(cudaStream_t stream) {
+  NNB_CUFFT(cufftSetStream(plan_, stream));
+  const int dir = sign_ < 0 ? CUFFT_FORWARD : CUFFT_INVERSE;
+  if constexpr (std::is_same<T, float>::value) {
+    NNB_CUFFT(cufftExecC2C(plan_, reinterpret_cast<cufftComplex*>(grid_.data()),
+                           reinterpret_cast<cufftComplex*>(grid_.data()), dir));
+  } else {
+    NNB_CUFFT(cufftExecZ2Z(plan_, reinterpret_cast<cufftDoubleComplex*>(grid_.data()),
+                           reinterpret_cast<cufftDoubleComplex*>(grid_.data()), dir));
+  }
+}
+
+template class FftGrid<float>;
+template class FftGrid<double>;
+
+// ---- point sets -------------------------------------------------------------------------------
+template <typename T>
+PointSet<T>::PointSet(std::shared_ptr<DeviceAllocator> alloc)
+    : perm_(alloc), local_(alloc), counts_(alloc), bin_start_(alloc), ranks_(alloc),
+      scan_tmp_(alloc), err_(alloc) {
+  for (auto& f : frac_) f.set_allocator(alloc);
+}
+
+template <typename T>
+void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream) {
+  if (M < 0) throw_input("negative number of points");
+  if (M > i64(0xffffffffll)) throw_input("more than 2^32 - 1 points per plan");
+  for (int d = 0; d < g.dim && M > 0; ++d) {
+    if (!x.p[d]) throw_input("null coordinate pointer");
+  }
+  g_ = g;
+  M_ = M;
+  const i64 nt = g.total_tiles;
+  counts_.reserve(size_t(nt));
+  bin_start_.reserve(size_t(nt + 1));
+  scan_tmp_.reserve(size_t(scan_tmp_words(nt)));
+  perm_.reserve(size_t(M));
+  local_.reserve(size_t(M));
+  ranks_.reserve(size_t(M));
+  for (int d = 0; d < 3; ++d) {
+    if (d < g.dim) {
+      frac_[d].reserve(size_t(M));
+    } else {
+      frac_[d].release();
+    }
+  }
+  err_.reserve(1);
+  NNB_CUDA(cudaMemsetAsync(counts_.data(), 0, sizeof(u32) * nt, stream));
+  NNB_CUDA(cudaMemsetAsync(err_.data(), 0, sizeof(int), stream));
+  launch_bin_count<T>(g, x, M, counts_.data(), ranks_.data(), err_.data(), stream);
+  launch_exclusive_scan(counts_.data(), bin_start_.data(), nt, scan_tmp_.data(), stream);
+  launch_bin_scatter<T, T>(g, x, M, ranks_.data(), bin_start_.data(), perm_.data(),
+                           local_.data(), frac_[0].data(), frac_[1].data(), frac_[2].data(),
+                           stream);
+  int host_err = 0;
+  NNB_CUDA(cudaMemcpyAsync(&host_err, err_.data(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+  NNB_CUDA(cudaStreamSynchronize(stream));
+  if (host_err) {
+    M_ = 0;
+    throw_input("non-finite point coordinate");
+  }
+}
+
+template <typename T>
+SortedPoints<T> PointSet<T>::view() const {
+  SortedPoints<T> v;
+  v.perm = perm_.data();
+  v.local = local_.data();
+  for (int d = 0; d < 3; ++d) v.frac[d] = frac_[d].data();
+  v.bin_start = bin_start_.data();
+  return v;
+}
+
+template class PointSet<float>;
+template class PointSet<double>;
+
+// ---- tiles ----------------------------------------------------------------------------------------
+void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int* requested,
+                 int* tile) {
+  const int max_bits[3] = {dim == 3 ? 11 : (dim == 2 ? 16 : 31), dim == 3 ? 11 : 16, 10};
+  bool explicit_tile = requested && requested[0] > 0;
+  for (int d = 0; d < 3; ++d) tile[d] = 1;
+  if (explicit_tile) {
+    for (int d = 0; d < dim; ++d) {
+      const int t = requested[d];
+      if (t < 1 || (max_bits[d] < 31 && t > (1 << max_bits[d]))) throw_input("invalid tile shape");
+      tile[d] = t;
+    }
+  } else {
+    if (dim == 1) {
+      tile[0] = 1024;
+    } else if (dim == 2) {
+      tile[0] = 32;
+      tile[1] = 32;
+    } else {
+      tile[0] = 16;
+      tile[1] = 8;
+      tile[2] = 8;
+    }
+    // Shrink the largest tile dimension until the padded tile fits the shared-memory budget.
+    const size_t budget = 96 * 1024;
+    for (;;) {
+      size_t cells = 1;
+      for (int d = 0; d < dim; ++d) cells *= size_t(tile[d] + w - 1);
+      if (cells * complex_bytes <= budget) break;
+      int big = 0;
+      for (int d = 1; d < dim; ++d) {
+        if (tile[d] > tile[big]) big = d;
+      }
+      if (tile[big] <= 1) break;
+      tile[big] /= 2;
+    }
+  }
+  for (int d = 0; d < dim; ++d) {
+    if (tile[d] > nf[d]) tile[d] = int(nf[d]);
+  }
+  size_t cells = 1;
+  for (int d = 0; d < dim; ++d) cells *= size_t(tile[d] + w - 1);
+  if (cells * complex_bytes > 200 * 1024) throw_input("tile too large for shared memory");
+}
+
+BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* offset,
+                  const double* scale) {
+  BinGeom g{};
+  g.dim = dim;
+  g.w = w;
+  g.total_tiles = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (d < dim) {
+      g.nf[d] = nf[d];
+      g.tile[d] = tile[d];
+      g.ntiles[d] = int((nf[d] + tile[d] - 1) / tile[d]);
+      g.offset[d] = offset ? offset[d] : 0.0;
+      g.scale[d] = scale ? scale[d] : 1.0;
+    } else {
+      g.nf[d] = 1;
+      g.tile[d] = 1;
+      g.ntiles[d] = 1;
+      g.offset[d] = 0.0;
+      g.scale[d] = 1.0;
+    }
+    g.total_tiles *= g.ntiles[d];
+  }
+  if (g.total_tiles > i64(0x7fffffff)) throw_input("too many tiles");
+  return g;
+}
+
+}  // namespace nnb

@@ -1,0 +1,160 @@
+// Host runtime pieces: allocator adapter, owning device arrays, cuFFT grid, stage timer,
+// bin-sorted point sets. Used by the plan implementations (plan.cu).
+#pragma once
+
+#include <atomic>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "neonufft_gpu.h"
+#include "params.hpp"
+
+namespace nnb {
+
+// Number of engine kernels launched by this process (all plans, all devices).
+extern std::atomic<i64> g_kernel_launches;
+
+// Adapter over the user's NnbAllocator (or cudaMalloc / cudaFree when none is given).
+class DeviceAllocator {
+public:
+  explicit DeviceAllocator(const NnbAllocator* a);
+  void* allocate(size_t bytes);  // throws MemoryAllocError
+  void deallocate(void* p, size_t bytes) noexcept;
+  u64 in_use() const { return in_use_; }
+
+private:
+  NnbAllocator a_{};
+  bool custom_ = false;
+  u64 in_use_ = 0;
+};
+
+// Owning device array allocated through the plan's allocator.
+template <typename X>
+class DevArray {
+public:
+  DevArray() = default;
+  explicit DevArray(std::shared_ptr<DeviceAllocator> alloc) : alloc_(std::move(alloc)) {}
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  ~DevArray() { release(); }
+
+  void set_allocator(std::shared_ptr<DeviceAllocator> alloc) { alloc_ = std::move(alloc); }
+
+  // Ensures capacity for n elements (reallocates only when growing).
+  void reserve(size_t n) {
+    if (n <= cap_) {
+      n_ = n;
+      return;
+    }
+    release();
+    if (n) ptr_ = static_cast<X*>(alloc_->allocate(n * sizeof(X)));
+    cap_ = n;
+    n_ = n;
+  }
+  void release() {
+    if (ptr_) alloc_->deallocate(ptr_, cap_ * sizeof(X));
+    ptr_ = nullptr;
+    cap_ = n_ = 0;
+  }
+  X* data() const { return ptr_; }
+  size_t size() const { return n_; }
+
+private:
+  std::shared_ptr<DeviceAllocator> alloc_;
+  X* ptr_ = nullptr;
+  size_t cap_ = 0;
+  size_t n_ = 0;
+};
+
+// Records CUDA events around plan stages when enabled; sums elapsed times on request.
+class StageTimer {
+public:
+  ~StageTimer();
+  void enable(bool on) { enabled_ = on; }
+  bool enabled() const { return enabled_; }
+  void begin(cudaStream_t s, int stage);
+  void end(cudaStream_t s, int stage);
+  void collect(cudaStream_t s, double* ms, i64* count, bool reset);
+
+private:
+  cudaEvent_t get_event();
+  struct Pending {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  bool enabled_ = false;
+  int open_stage_ = -1;
+  cudaEvent_t open_event_ = nullptr;
+  std::vector<Pending> pending_;
+  std::vector<cudaEvent_t> pool_;
+  double ms_[NNB_STAGE_COUNT] = {0};
+  i64 count_[NNB_STAGE_COUNT] = {0};
+};
+
+class ScopedStage {
+public:
+  ScopedStage(StageTimer& t, cudaStream_t s, int stage) : t_(t), s_(s), stage_(stage) {
+    t_.begin(s_, stage_);
+  }
+  ~ScopedStage() { t_.end(s_, stage_); }
+
+private:
+  StageTimer& t_;
+  cudaStream_t s_;
+  int stage_;
+};
+
+// Complex fine grid with an in-place cuFFT plan (workspace from the plan's allocator).
+// Replaces the reference's FFTGrid (src/neonufft/gpu/util/fft_grid.cpp:19-70).
+template <typename T>
+class FftGrid {
+public:
+  FftGrid(std::shared_ptr<DeviceAllocator> alloc, int dim, const i64* nf, int sign,
+          cudaStream_t stream);
+  ~FftGrid();
+  void exec(cudaStream_t stream);
+  cplx_t<T>* data() const { return grid_.data(); }
+  i64 cells() const { return cells_; }
+  const i64* nf() const { return nf_; }
+
+private:
+  DevArray<cplx_t<T>> grid_;
+  DevArray<unsigned char> work_;
+  cufftHandle plan_ = 0;
+  bool has_plan_ = false;
+  int dim_;
+  int sign_;
+  i64 nf_[3] = {1, 1, 1};
+  i64 cells_ = 1;
+};
+
+// Bin-sorted point set on one fine grid (see binning.cu).
+template <typename T>
+class PointSet {
+public:
+  explicit PointSet(std::shared_ptr<DeviceAllocator> alloc);
+  // Bins M points; enqueues work on `stream`, then synchronises it and throws InputError for
+  // non-finite coordinates.
+  void build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream);
+  SortedPoints<T> view() const;
+  i64 size() const { return M_; }
+  const BinGeom& geom() const { return g_; }
+
+private:
+  BinGeom g_{};
+  i64 M_ = 0;
+  DevArray<u32> perm_, local_, counts_, bin_start_, ranks_, scan_tmp_;
+  DevArray<T> frac_[3];
+  DevArray<int> err_;
+};
+
+// Tile shape for a grid: explicit request (validated) or the automatic choice.
+void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int* requested,
+                 int* tile);
+
+BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* offset,
+                  const double* scale);
+
+}  // namespace nnb
