@@ -57,8 +57,9 @@ typedef struct NnbOptions {
   int order;                /* NeonufftModeOrder */
   int kernel_type;          /* NeonufftKernelType */
   int tile[3];              /* subproblem tile (bin) shape in fine-grid cells; 0 = automatic */
-  int spread_method;        /* 0 = automatic; see nnb_plan_info */
-  int reserved[8];
+  int spread_method;        /* 0 = automatic; 1 = warp-private slabs; 2 = thread per point */
+  int n_spread;             /* kernel width override in [2, 16]; 0 = the reference heuristic */
+  int reserved[7];
 } NnbOptions;
 
 /* Fills *opt with the reference defaults (tol 1e-3, upsampfac 2, recenter 0.1, CMCL). */

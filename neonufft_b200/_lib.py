@@ -24,7 +24,8 @@ class NnbOptions(C.Structure):
         ("tol", C.c_double), ("upsampfac", C.c_double), ("recenter_threshold", C.c_double),
         ("num_threads", C.c_int), ("sort_input", C.c_int), ("sort_output", C.c_int),
         ("kernel_approximation", C.c_int), ("order", C.c_int), ("kernel_type", C.c_int),
-        ("tile", C.c_int * 3), ("spread_method", C.c_int), ("reserved", C.c_int * 8),
+        ("tile", C.c_int * 3), ("spread_method", C.c_int), ("n_spread", C.c_int),
+        ("reserved", C.c_int * 7),
     ]
 
 

@@ -291,7 +291,7 @@ NeonufftError nnb_plan_t3_geometry(NnbPrecision precision, int dim, const NnbOpt
     need(output_min, "bounds");
     need(output_max, "bounds");
     const bool single = precision == NNB_FLOAT;
-    const nnb::KernelParam kp = nnb::kernel_param(o.tol, o.upsampfac, single);
+    const nnb::KernelParam kp = nnb::kernel_param(o.tol, o.upsampfac, single, o.n_spread);
     for (int d = 0; d < dim; ++d) {
       int64_t nf1, nfft;
       double C, D, g, hh;

@@ -134,4 +134,19 @@ __device__ __forceinline__ double es_eval<double>(double x, double beta, double 
   return arg > 0.0 ? exp(beta * (sqrt(arg) - 1.0)) : 0.0;
 }
 
+// Fast ES kernel for the hot loops: single precision uses the hardware exponential
+// (__expf); double precision is the same as es_eval.
+template <typename T>
+__device__ __forceinline__ T es_eval_fast(T x, T beta, T c);
+
+template <>
+__device__ __forceinline__ float es_eval_fast<float>(float x, float beta, float c) {
+  const float arg = 1.f - c * x * x;
+  return arg > 0.f ? __expf(beta * (sqrtf(arg) - 1.f)) : 0.f;
+}
+template <>
+__device__ __forceinline__ double es_eval_fast<double>(double x, double beta, double c) {
+  return es_eval<double>(x, beta, c);
+}
+
 }  // namespace nnb

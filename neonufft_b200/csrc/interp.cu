@@ -1,125 +1,289 @@
 // ES interpolation by shared-memory subproblem tiles.
 //
 // Replaces the reference's interpolation (src/neonufft/gpu/kernels/interpolation_kernel.cu:27-457),
-// where each warp gathers its point's w^d cells straight from global memory in the user's
-// point order. Here one CTA owns one tile: the tile plus its (w-1)-cell halo is staged once
-// into shared memory (coalesced along x, periodic wrap), then each warp takes the tile's
-// bin-sorted points one at a time: lanes evaluate the w*d kernel values, sweep the footprint
-// in shared memory, and reduce with shuffles. The optional per-point factor (type-3 postphase)
-// is applied before the result is written to the point's original position.
+// where each warp gathers its point's w^d cells straight from global memory in the user's point
+// order.
+//
+// Method 1 (default): a CTA of up to 4 warps covers as many consecutive tiles (bins) along the
+// last dimension and stages their union plus the (w-1)-cell halo into shared memory once
+// (coalesced along x, periodic wrap, padded strides, tile_layout.cuh). Each warp walks one
+// tile's bin-sorted points in batches of 32 (lane j loads point j's record and evaluates its
+// w*d kernel values, all in parallel); then, one point at a time, lane r contracts footprint
+// row r (3D: (dy, dz); 2D: cell (dx, dy)) against kx, and a shuffle reduction forms the
+// point's value, which lane j applies the optional per-point factor to (type-3 postphase) and
+// stores at the point's original index.
+// Method 2: thread per point on one staged tile per CTA.
 #include "kernels.cuh"
+#include "tile_layout.cuh"
 
 namespace nnb {
 
 namespace {
 
-constexpr int kInterpThreads = 256;
-constexpr int kKerStride = 16;
+constexpr int kMaxInterpWarps = 4;  // warps (tiles) per CTA; fewer when the region does not fit
+constexpr int kTppThreads = 256;
 
-template <int W, int DIM>
-struct Footprint {
-  static constexpr int cells = (DIM == 1) ? W : (DIM == 2 ? W * W : W * W * W);
-};
+// Stages rows [0, nrows) of the padded region starting at (o0, o1, o2) (3D rows are (cy, cz)
+// pairs, 2D rows are cy, 1D has one row of ext cells), with periodic wrap.
+template <typename T, int DIM>
+__device__ __forceinline__ void stage_region(const BinGeom& g, const TileLayout& L, int nrows,
+                                             int ext1d, i64 o0, i64 o1, i64 o2,
+                                             const cplx_t<T>* grid, cplx_t<T>* tile) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  if (DIM == 1) {
+    for (int cx = threadIdx.x; cx < ext1d; cx += blockDim.x) {
+      tile[cx] = grid[wrap_index(o0 + cx, g.nf[0])];
+    }
+    return;
+  }
+  for (int row = warp; row < nrows; row += nwarps) {
+    int cy = row, cz = 0;
+    if (DIM == 3) {
+      cz = row / L.P1;
+      cy = row - cz * L.P1;
+    }
+    i64 rbase = wrap_index(o1 + cy, g.nf[1]) * g.nf[0];
+    if (DIM == 3) rbase += wrap_index(o2 + cz, g.nf[2]) * g.nf[0] * g.nf[1];
+    cplx_t<T>* dst = tile + cz * L.PS + cy * L.RS;
+    for (int cx = lane; cx < L.P0; cx += 32) dst[cx] = grid[rbase + wrap_index(o0 + cx, g.nf[0])];
+  }
+}
 
 template <typename T, int DIM, int W>
-__global__ void __launch_bounds__(kInterpThreads) interp_tiles_kernel(InterpArgs<T> a) {
+__global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(InterpArgs<T> a,
+                                                                           TileLayout L) {
   using C = cplx_t<T>;
+  const int nwarps = blockDim.x >> 5;
+  constexpr int KS = (DIM * W) | 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  T* kbuf = reinterpret_cast<T*>(tile + L.cells);
 
   const BinGeom& g = a.g;
-  const i64 bin = blockIdx.x;
-  const u32 start = a.pts.bin_start[bin];
-  const u32 end = a.pts.bin_start[bin + 1];
-  if (start == end) return;
-
-  const int P0 = g.tile[0] + W - 1;
-  const int P1 = DIM > 1 ? g.tile[1] + W - 1 : 1;
-  const int P2 = DIM > 2 ? g.tile[2] + W - 1 : 1;
-  const int ncell = P0 * P1 * P2;
-
-  C* tile = reinterpret_cast<C*>(smem_raw);
-  T* kbuf = reinterpret_cast<T*>(tile + ncell);
-
-  const i64 t0 = bin % g.ntiles[0];
-  const i64 t1 = DIM > 1 ? (bin / g.ntiles[0]) % g.ntiles[1] : 0;
-  const i64 t2 = DIM > 2 ? bin / (i64(g.ntiles[0]) * g.ntiles[1]) : 0;
-  const i64 o0 = t0 * g.tile[0], o1 = t1 * g.tile[1], o2 = t2 * g.tile[2];
-
-  for (int i = threadIdx.x; i < ncell; i += kInterpThreads) {
-    const int cx = i % P0;
-    const int r = i / P0;
-    const int cy = r % P1;
-    const int cz = r / P1;
-    i64 gx = o0 + cx;
-    while (gx >= g.nf[0]) gx -= g.nf[0];
-    i64 gidx = gx;
-    if (DIM > 1) {
-      i64 gy = o1 + cy;
-      while (gy >= g.nf[1]) gy -= g.nf[1];
-      gidx += gy * g.nf[0];
+  constexpr int LD = DIM - 1;
+  const int n_last = g.ntiles[LD];
+  const int groups = (n_last + nwarps - 1) / nwarps;
+  const i64 rest = blockIdx.x / groups;
+  const int grp = int(blockIdx.x - rest * groups);
+  int tc[3] = {0, 0, 0};
+  {
+    i64 r = rest;
+    for (int d = 0; d < LD; ++d) {
+      tc[d] = int(r % g.ntiles[d]);
+      r /= g.ntiles[d];
     }
-    if (DIM > 2) {
-      i64 gz = o2 + cz;
-      while (gz >= g.nf[2]) gz -= g.nf[2];
-      gidx += gz * g.nf[0] * g.nf[1];
-    }
-    tile[i] = a.grid[gidx];
+    tc[LD] = grp * nwarps;
   }
-  __syncthreads();
+  const int T_last = g.tile[LD];
+  int nvalid = n_last - tc[LD];
+  if (nvalid > nwarps) nvalid = nwarps;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  constexpr int nwarps = kInterpThreads / 32;
-  T* kv = kbuf + warp * (DIM * kKerStride);
+  auto bin_of = [&](int t_last) -> i64 {
+    if (DIM == 1) return t_last;
+    if (DIM == 2) return tc[0] + i64(g.ntiles[0]) * t_last;
+    return tc[0] + i64(g.ntiles[0]) * (tc[1] + i64(g.ntiles[1]) * t_last);
+  };
+  // Skip CTAs without points (no staging traffic).
+  bool any = false;
+  for (int w = 0; w < nvalid; ++w) {
+    const i64 b = bin_of(tc[LD] + w);
+    any |= a.pts.bin_start[b + 1] > a.pts.bin_start[b];
+  }
+  if (!any) return;
 
-  for (u32 p = start + warp; p < end; p += nwarps) {
-    for (int j = lane; j < DIM * W; j += 32) {
-      const int d = j / W;
-      const int k = j - d * W;
-      kv[d * kKerStride + k] = es_eval<T>(a.pts.frac[d][p] + T(k), a.beta, a.c);
-    }
-    int lx, ly, lz;
-    unpack_local(DIM, a.pts.local[p], lx, ly, lz);
-    __syncwarp();
-    T sx = 0, sy = 0;
-    for (int k = lane; k < Footprint<W, DIM>::cells; k += 32) {
-      const int dx = k % W;
-      const int r = k / W;
-      const int dy = DIM > 1 ? r % W : 0;
-      const int dz = DIM > 2 ? r / W : 0;
-      T kval = kv[dx];
-      if (DIM > 1) kval *= kv[kKerStride + dy];
-      if (DIM > 2) kval *= kv[2 * kKerStride + dz];
-      const C gv = tile[((lz + dz) * P1 + (ly + dy)) * P0 + (lx + dx)];
-      sx += kval * gv.x;
-      sy += kval * gv.y;
-    }
+  const i64 o0 = i64(tc[0]) * g.tile[0];
+  const i64 o1 = DIM > 1 ? i64(tc[1]) * g.tile[1] : 0;
+  const i64 o2 = DIM > 2 ? i64(tc[2]) * g.tile[2] : 0;
+  const int p_last = nvalid * T_last + W - 1;  // staged extent along the last dimension
+  stage_region<T, DIM>(g, L, DIM == 3 ? p_last * L.P1 : p_last, p_last, o0, o1, o2, a.grid,
+                       tile);
+  __syncthreads();
+
+  if (warp >= nvalid) return;
+  const i64 bin = bin_of(tc[LD] + warp);
+  const u32 start = a.pts.bin_start[bin];
+  const u32 end = a.pts.bin_start[bin + 1];
+  T* kvb = kbuf + warp * 32 * KS;
+  const int shift = warp * T_last * ((DIM == 3) ? L.PS : (DIM == 2 ? L.RS : 1));
+
+  constexpr int NR = (DIM == 1) ? W : W * W;
+  constexpr int PASSES = (NR + 31) / 32;
+  int roff[PASSES], ra[PASSES], rb[PASSES];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sx += __shfl_xor_sync(0xffffffffu, sx, o);
-      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  for (int k = 0; k < PASSES; ++k) {
+    const int r = lane + 32 * k;
+    ra[k] = r % W;
+    rb[k] = r / W;
+    if (DIM == 3) roff[k] = rb[k] * L.PS + ra[k] * L.RS;
+    else if (DIM == 2) roff[k] = rb[k] * L.RS + ra[k];
+    else roff[k] = r;
+  }
+
+  for (u32 b = start; b < end; b += 32) {
+    const u32 nb = (end - b) < 32u ? (end - b) : 32u;
+    int my_base = 0;
+    u32 my_idx = 0;
+    C my_post{T(1), T(0)};
+    if (lane < nb) {
+      const u32 p = b + lane;
+      my_idx = a.pts.perm[p];
+      if (a.postphase) my_post = a.postphase[my_idx];
+      int lx, ly, lz;
+      unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+      my_base = shift + lz * L.PS + ly * L.RS + lx;
+      T* kr = kvb + lane * KS;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const T f = a.pts.frac[d][p];
+#pragma unroll
+        for (int k = 0; k < W; ++k) kr[d * W + k] = es_eval_fast<T>(f + T(k), a.beta, a.c);
+      }
     }
-    if (lane == 0) {
-      const u32 idx = a.pts.perm[p];
-      C res{sx, sy};
-      if (a.postphase) res = cmul(res, a.postphase[idx]);
-      a.out[idx] = res;
+    __syncwarp();
+    for (u32 j = 0; j < nb; ++j) {
+      const int base = __shfl_sync(0xffffffffu, my_base, int(j));
+      const T* kj = kvb + j * KS;
+      T sx = 0, sy = 0;
+      if (DIM == 3) {
+        T kx[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) kx[k] = kj[k];
+#pragma unroll
+        for (int k = 0; k < PASSES; ++k) {
+          if (lane + 32 * k < NR) {
+            const C* row = tile + base + roff[k];
+            T rx = 0, ry = 0;
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) {
+              const C gv = row[dx];
+              rx += kx[dx] * gv.x;
+              ry += kx[dx] * gv.y;
+            }
+            const T kyz = kj[W + ra[k]] * kj[2 * W + rb[k]];
+            sx += kyz * rx;
+            sy += kyz * ry;
+          }
+        }
+      } else if (DIM == 2) {
+#pragma unroll
+        for (int k = 0; k < PASSES; ++k) {
+          if (lane + 32 * k < NR) {
+            const T kk = kj[ra[k]] * kj[W + rb[k]];
+            const C gv = tile[base + roff[k]];
+            sx += kk * gv.x;
+            sy += kk * gv.y;
+          }
+        }
+      } else {
+        if (lane < W) {
+          const C gv = tile[base + lane];
+          sx = kj[lane] * gv.x;
+          sy = kj[lane] * gv.y;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+      }
+      if (lane == int(j)) {
+        C res{sx, sy};
+        if (a.postphase) res = cmul(res, my_post);
+        a.out[my_idx] = res;
+      }
     }
     __syncwarp();
   }
 }
 
+// Thread-per-point variant on one staged tile per CTA.
+template <typename T, int DIM, int W>
+__global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a, TileLayout L) {
+  using C = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  const BinGeom& g = a.g;
+  const i64 bin = blockIdx.x;
+  const u32 start = a.pts.bin_start[bin];
+  const u32 end = a.pts.bin_start[bin + 1];
+  if (start == end) return;
+  const i64 t0 = bin % g.ntiles[0];
+  const i64 t1 = DIM > 1 ? (bin / g.ntiles[0]) % g.ntiles[1] : 0;
+  const i64 t2 = DIM > 2 ? bin / (i64(g.ntiles[0]) * g.ntiles[1]) : 0;
+  stage_region<T, DIM>(g, L, DIM == 3 ? L.P1 * L.P2 : L.P1, L.P0, t0 * g.tile[0],
+                       t1 * g.tile[1], t2 * g.tile[2], a.grid, tile);
+  __syncthreads();
+  for (u32 p = start + threadIdx.x; p < end; p += kTppThreads) {
+    int lx, ly, lz;
+    unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+    T kx[W];
+    const T fx = a.pts.frac[0][p];
+#pragma unroll
+    for (int k = 0; k < W; ++k) kx[k] = es_eval_fast<T>(fx + T(k), a.beta, a.c);
+    T sx = 0, sy = 0;
+    const int nz = DIM > 2 ? W : 1;
+    const int ny = DIM > 1 ? W : 1;
+    const T fy = DIM > 1 ? a.pts.frac[1][p] : T(0);
+    const T fz = DIM > 2 ? a.pts.frac[2][p] : T(0);
+#pragma unroll 1
+    for (int dz = 0; dz < nz; ++dz) {
+      const T kz = DIM > 2 ? es_eval_fast<T>(fz + T(dz), a.beta, a.c) : T(1);
+#pragma unroll 1
+      for (int dy = 0; dy < ny; ++dy) {
+        const T ky = (DIM > 1 ? es_eval_fast<T>(fy + T(dy), a.beta, a.c) : T(1)) * kz;
+        const C* row = tile + (lz + dz) * L.PS + (ly + dy) * L.RS + lx;
+        T rx = 0, ry = 0;
+#pragma unroll
+        for (int dx = 0; dx < W; ++dx) {
+          const C gv = row[dx];
+          rx += kx[dx] * gv.x;
+          ry += kx[dx] * gv.y;
+        }
+        sx += ky * rx;
+        sy += ky * ry;
+      }
+    }
+    const u32 idx = a.pts.perm[p];
+    C res{sx, sy};
+    if (a.postphase) res = cmul(res, a.postphase[idx]);
+    a.out[idx] = res;
+  }
+}
+
 template <typename T, int DIM, int W>
 void launch_interp_tw(const InterpArgs<T>& a, cudaStream_t stream) {
-  const int P0 = a.g.tile[0] + W - 1;
-  const int P1 = DIM > 1 ? a.g.tile[1] + W - 1 : 1;
-  const int P2 = DIM > 2 ? a.g.tile[2] + W - 1 : 1;
-  const size_t smem = size_t(P0) * P1 * P2 * sizeof(cplx_t<T>) +
-                      size_t(kInterpThreads / 32) * DIM * kKerStride * sizeof(T);
+  const int LD = DIM - 1;
+  if (a.method == 2) {
+    const TileLayout L = make_tile_layout(DIM, W, a.g.tile[0], a.g.tile[1], a.g.tile[2],
+                                          int(sizeof(cplx_t<T>)));
+    const size_t smem = size_t(L.cells) * sizeof(cplx_t<T>);
+    if (smem > 227 * 1024) throw_internal("interpolation tile does not fit in shared memory");
+    auto kern = interp_tpp_kernel<T, DIM, W>;
+    NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<unsigned(a.g.total_tiles), kTppThreads, smem, stream>>>(a, L);
+    NNB_LAUNCH_CHECK();
+    return;
+  }
+  int nw = kMaxInterpWarps;
+  TileLayout L{};
+  size_t smem = 0;
+  for (;; nw /= 2) {
+    int ext[3] = {a.g.tile[0], a.g.tile[1], a.g.tile[2]};
+    ext[LD] = nw * a.g.tile[LD];
+    L = make_tile_layout(DIM, W, ext[0], ext[1], ext[2], int(sizeof(cplx_t<T>)));
+    smem = size_t(L.cells) * sizeof(cplx_t<T>) + size_t(nw) * 32 * ((DIM * W) | 1) * sizeof(T);
+    if (smem <= 227 * 1024 || nw == 1) break;
+  }
   if (smem > 227 * 1024) throw_internal("interpolation tile does not fit in shared memory");
-  auto kern = interp_tiles_kernel<T, DIM, W>;
+  auto kern = interp_slab_kernel<T, DIM, W>;
   NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  kern<<<unsigned(a.g.total_tiles), kInterpThreads, smem, stream>>>(a);
+  const i64 groups = (a.g.ntiles[LD] + nw - 1) / nw;
+  const i64 ctas = a.g.total_tiles / a.g.ntiles[LD] * groups;
+  kern<<<unsigned(ctas), nw * 32, smem, stream>>>(a, L);
   NNB_LAUNCH_CHECK();
 }
 
@@ -146,6 +310,14 @@ void launch_interp_d(const InterpArgs<T>& a, cudaStream_t stream) {
 }
 
 }  // namespace
+
+size_t interp_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps) {
+  int ext[3] = {tile[0], dim > 1 ? tile[1] : 1, dim > 2 ? tile[2] : 1};
+  ext[dim - 1] *= warps;
+  const TileLayout L = make_tile_layout(dim, w, ext[0], ext[1], ext[2], int(complex_bytes));
+  return size_t(L.cells) * complex_bytes +
+         size_t(warps) * 32 * ((dim * w) | 1) * (complex_bytes / 2);
+}
 
 template <typename T>
 void launch_interp(const InterpArgs<T>& a, cudaStream_t stream) {

@@ -38,9 +38,13 @@ struct SpreadArgs {
   int batch;
   T beta;
   T c;
+  int method;  // 1: warp per point, 2: thread per point
 };
 template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream);
+// Dynamic shared memory of the default spreading / interpolation kernels for a tile shape.
+size_t spread_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
+size_t interp_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
 
 // ---- interpolation (interp.cu) --------------------------------------------------------------
 template <typename T>
@@ -52,6 +56,7 @@ struct InterpArgs {
   cplx_t<T>* out;              // original point order
   T beta;
   T c;
+  int method;  // 1: warp per point, 2: thread per point
 };
 template <typename T>
 void launch_interp(const InterpArgs<T>& a, cudaStream_t stream);

@@ -11,7 +11,7 @@ namespace {
 constexpr double kPiD = 3.14159265358979323846264338327950288;
 }
 
-KernelParam kernel_param(double tol, double upsampfac, bool single) {
+KernelParam kernel_param(double tol, double upsampfac, bool single, int w_override) {
   // Width heuristic and beta factors of the reference (src/neonufft/es_kernel_param.hpp:27-55):
   // w = ceil(-log10(tol/10)) for upsampfac 2, else ceil(-ln(tol) / (pi sqrt(1 - 1/upsampfac))),
   // clamped to [2, 16]; beta = f(w) * w with FINUFFT's factors, or Eq. 4.5 of the FINUFFT paper
@@ -24,6 +24,7 @@ KernelParam kernel_param(double tol, double upsampfac, bool single) {
   }
   w = std::max(2, w);
   w = std::min(16, w);
+  if (w_override >= 2 && w_override <= 16) w = w_override;
 
   double beta_fac = 2.30;
   if (w == 2) beta_fac = 2.20;

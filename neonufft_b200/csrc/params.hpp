@@ -24,7 +24,8 @@ struct KernelParam {
 };
 
 // `single` selects rounding of beta and c to float (the reference stores them as T).
-KernelParam kernel_param(double tol, double upsampfac, bool single);
+// `w_override` in [2, 16] replaces the width heuristic (beta then follows the same rule).
+KernelParam kernel_param(double tol, double upsampfac, bool single, int w_override = 0);
 
 // Fine grid size of a type-1/2 plan along one dimension: max(2w, floor(modes * upsampfac)).
 std::int64_t fine_grid_size(std::int64_t modes, double upsampfac, int w);

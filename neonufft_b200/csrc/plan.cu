@@ -9,6 +9,9 @@ namespace nnb {
 
 namespace {
 
+// Default spreading / interpolation method (see spread.cu and interp.cu).
+constexpr int kDefaultMethod = 1;
+
 template <typename T>
 constexpr bool is_single() {
   return std::is_same<T, float>::value;
@@ -55,6 +58,10 @@ void validate_options(const NnbOptions& opt) {
   for (int d = 0; d < 3; ++d) {
     if (opt.tile[d] < 0) throw_input("invalid tile shape");
   }
+  if (opt.spread_method < 0 || opt.spread_method > 2) throw_input("invalid spread method");
+  if (opt.n_spread != 0 && (opt.n_spread < 2 || opt.n_spread > 16)) {
+    throw_input("kernel width must be in [2, 16]");
+  }
 }
 
 // =============================================================================================
@@ -80,8 +87,9 @@ public:
       if (modes[d] < 1) throw_input("number of modes must be positive");
       modes_[d] = modes[d];
     }
-    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
+    if (opt.spread_method > 0) method_ = opt.spread_method;
     for (int d = 0; d < dim; ++d) nf_[d] = fine_grid_size(modes_[d], opt.upsampfac, kp_.w);
     fft_ = std::make_unique<FftGrid<T>>(alloc_, dim, nf_, sign_, stream_);
     for (int d = 0; d < dim; ++d) {
@@ -120,6 +128,7 @@ public:
         a.batch = 1;
         a.beta = T(kp_.beta);
         a.c = T(kp_.c);
+        a.method = method_;
         launch_spread<T>(a, stream_);
       }
     }
@@ -158,6 +167,7 @@ public:
       a.out = static_cast<cplx_t<T>*>(out);
       a.beta = T(kp_.beta);
       a.c = T(kp_.c);
+      a.method = method_;
       launch_interp<T>(a, stream_);
     }
   }
@@ -167,7 +177,7 @@ public:
     info->dim = dim_;
     info->precision = is_single<T>() ? NNB_FLOAT : NNB_DOUBLE;
     info->n_spread = kp_.w;
-    info->spread_method = 1;
+    info->spread_method = method_;
     info->es_beta = kp_.beta;
     for (int d = 0; d < 3; ++d) {
       info->grid[d] = nf_[d];
@@ -206,6 +216,7 @@ private:
   i64 modes_[3];
   i64 nf_[3];
   int tile_[3] = {1, 1, 1};
+  int method_ = kDefaultMethod;
   BinGeom geom_{};
   std::unique_ptr<FftGrid<T>> fft_;
   DevArray<T> corr_[3];
@@ -234,8 +245,9 @@ public:
         out_points_(alloc_) {
     if (batch < 1) throw_input("batch size must be positive");
     if (batch > 65535) throw_input("batch size above 65535");
-    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+    kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
+    if (opt.spread_method > 0) method_ = opt.spread_method;
     for (auto& c : corr_) c.set_allocator(alloc_);
   }
 
@@ -381,6 +393,7 @@ public:
     a.batch = int(batch_);
     a.beta = T(kp_.beta);
     a.c = T(kp_.c);
+    a.method = method_;
     launch_spread<T>(a, stream_);
   }
 
@@ -418,6 +431,7 @@ public:
       a.out = static_cast<cplx_t<T>*>(out) + b * bdist;
       a.beta = T(kp_.beta);
       a.c = T(kp_.c);
+      a.method = method_;
       launch_interp<T>(a, stream_);
     }
   }
@@ -432,7 +446,7 @@ public:
     info->dim = dim_;
     info->precision = is_single<T>() ? NNB_FLOAT : NNB_DOUBLE;
     info->n_spread = kp_.w;
-    info->spread_method = 1;
+    info->spread_method = method_;
     info->es_beta = kp_.beta;
     for (int d = 0; d < 3; ++d) {
       info->grid[d] = nfft_[d];
@@ -466,6 +480,7 @@ private:
   double gamma_[3] = {1, 1, 1}, h_[3] = {1, 1, 1};
   int in_tile_[3] = {1, 1, 1};
   int out_tile_[3] = {1, 1, 1};
+  int method_ = kDefaultMethod;
   i64 spread_cells_ = 0;
   DevArray<cplx_t<T>> spread_grid_;
   std::unique_ptr<FftGrid<T>> fft_;
@@ -539,7 +554,7 @@ namespace {
 template <typename T>
 u64 t3_grid_bytes(int dim, const NnbOptions& opt, const double* in_min, const double* in_max,
                   const double* out_min, const double* out_max) {
-  const KernelParam kp = kernel_param(opt.tol, opt.upsampfac, is_single<T>());
+  const KernelParam kp = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
   u64 spread = 1, fft = 1;
   for (int d = 0; d < dim; ++d) {
     const T3Dim<T> g = t3_geometry<T>(kp.w, opt.upsampfac, T(opt.recenter_threshold),

@@ -265,36 +265,45 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
       tile[d] = t;
     }
   } else {
+    // Per-warp tile (bin); the kernels stack 4 of them along the last dimension per CTA.
     if (dim == 1) {
-      tile[0] = 1024;
+      tile[0] = 512;
     } else if (dim == 2) {
-      tile[0] = 32;
-      tile[1] = 32;
+      tile[0] = 64;
+      tile[1] = 16;
     } else {
-      tile[0] = 16;
+      tile[0] = 8;
       tile[1] = 8;
       tile[2] = 8;
     }
-    // Shrink the largest tile dimension until the padded tile fits the shared-memory budget.
-    const size_t budget = 96 * 1024;
+    // Shrink the largest tile dimension until both kernels fit two 4-warp CTAs per SM, but not
+    // below 4 cells (wide kernels then run with fewer warps per CTA), unless even one warp's
+    // slab would not fit.
+    const size_t budget = 113 * 1024;
     for (;;) {
-      size_t cells = 1;
-      for (int d = 0; d < dim; ++d) cells *= size_t(tile[d] + w - 1);
-      if (cells * complex_bytes <= budget) break;
+      for (int d = 0; d < dim; ++d) {
+        if (tile[d] > nf[d]) tile[d] = int(nf[d]);
+      }
+      const bool fits4 = spread_smem_bytes(dim, w, tile, complex_bytes, 4) <= budget &&
+                         interp_smem_bytes(dim, w, tile, complex_bytes, 4) <= budget;
+      const bool fits1 = spread_smem_bytes(dim, w, tile, complex_bytes, 1) <= 200 * 1024 &&
+                         interp_smem_bytes(dim, w, tile, complex_bytes, 1) <= 200 * 1024;
       int big = 0;
       for (int d = 1; d < dim; ++d) {
         if (tile[d] > tile[big]) big = d;
       }
-      if (tile[big] <= 1) break;
+      if (fits4 || (fits1 && tile[big] <= 4) || tile[big] <= 1) break;
       tile[big] /= 2;
     }
   }
   for (int d = 0; d < dim; ++d) {
     if (tile[d] > nf[d]) tile[d] = int(nf[d]);
   }
-  size_t cells = 1;
-  for (int d = 0; d < dim; ++d) cells *= size_t(tile[d] + w - 1);
-  if (cells * complex_bytes > 200 * 1024) throw_input("tile too large for shared memory");
+  // the kernels fall back to fewer warps per CTA; one warp must fit
+  if (spread_smem_bytes(dim, w, tile, complex_bytes, 1) > 227 * 1024 ||
+      interp_smem_bytes(dim, w, tile, complex_bytes, 1) > 227 * 1024) {
+    throw_input("tile too large for shared memory");
+  }
 }
 
 BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* offset,

@@ -64,7 +64,7 @@ def check(code: int) -> None:
 @dataclass
 class Options:
     """Mirror of neonufft::Options (reference include/neonufft/plan.hpp:19-29) plus engine
-    extensions (tile shape, spread method; 0 = automatic)."""
+    extensions (tile shape, spread method, kernel width override; 0 = automatic)."""
     tol: float = 0.001
     upsampfac: float = 2.0
     recenter_threshold: float = 0.1
@@ -76,6 +76,7 @@ class Options:
     kernel_type: int = 0
     tile: tuple = (0, 0, 0)
     spread_method: int = 0
+    n_spread: int = 0
 
     def to_c(self) -> L.NnbOptions:
         o = L.NnbOptions()
@@ -93,6 +94,7 @@ class Options:
         for i in range(3):
             o.tile[i] = int(t[i])
         o.spread_method = int(self.spread_method)
+        o.n_spread = int(self.n_spread)
         return o
 
 

@@ -11,6 +11,7 @@
 #include <array>
 #include <cstdint>
 #include <exception>
+#include <memory>
 
 #include "contrib/es_kernel/util.hpp"
 #include "contrib/legendre_rule/legendre_rule_fast.hpp"
@@ -85,6 +86,45 @@ void run3(const neonufft::Options& opt, int sign, int64_t M, const void* const* 
   cudaStreamSynchronize(nullptr);
 }
 
+// Persistent reference plan (for timing the reference GPU path without plan creation).
+struct RefPlan12Base {
+  virtual ~RefPlan12Base() = default;
+  virtual void set_points(int64_t M, const void* const* loc) = 0;
+  virtual void t1(const void* in, void* out, const int64_t* strides) = 0;
+  virtual void t2(const void* in, const int64_t* strides, void* out) = 0;
+};
+
+template <typename T, std::size_t D>
+struct RefPlan12 final : RefPlan12Base {
+  using CT = neonufft::gpu::ComplexType<T>;
+  std::unique_ptr<neonufft::gpu::Plan<T, D>> plan;
+  RefPlan12(const neonufft::Options& opt, int sign, int64_t M, const void* const* loc,
+            const int64_t* modes) {
+    std::array<const T*, D> l;
+    std::array<IntType, D> m;
+    for (std::size_t d = 0; d < D; ++d) {
+      l[d] = static_cast<const T*>(loc[d]);
+      m[d] = modes[d];
+    }
+    plan = std::make_unique<neonufft::gpu::Plan<T, D>>(opt, sign, M, l, m, nullptr);
+  }
+  void set_points(int64_t M, const void* const* loc) override {
+    std::array<const T*, D> l;
+    for (std::size_t d = 0; d < D; ++d) l[d] = static_cast<const T*>(loc[d]);
+    plan->set_points(M, l);
+  }
+  void t1(const void* in, void* out, const int64_t* strides) override {
+    std::array<IntType, D> s;
+    for (std::size_t d = 0; d < D; ++d) s[d] = strides[d];
+    plan->transform_type_1(static_cast<const CT*>(in), static_cast<CT*>(out), s);
+  }
+  void t2(const void* in, const int64_t* strides, void* out) override {
+    std::array<IntType, D> s;
+    for (std::size_t d = 0; d < D; ++d) s[d] = strides[d];
+    plan->transform_type_2(static_cast<const CT*>(in), s, static_cast<CT*>(out));
+  }
+};
+
 int code_of(const std::exception_ptr& e) {
   try {
     std::rethrow_exception(e);
@@ -153,6 +193,68 @@ __attribute__((visibility("default"))) int ref_gpu_type12(int is_float, int dim,
   } catch (...) {
     return code_of(std::current_exception());
   }
+}
+
+// Persistent reference type-1/2 plan on the legacy default stream: create, set points,
+// transform (asynchronous, as in the reference), destroy. Returns 0 or a NeonufftError code.
+__attribute__((visibility("default"))) int ref_plan12_create(void** handle, int is_float, int dim,
+                                                             double tol, double upsampfac,
+                                                             int sign, int64_t M,
+                                                             const void* const* loc,
+                                                             const int64_t* modes) {
+  try {
+    neonufft::Options opt;
+    opt.tol = tol;
+    opt.upsampfac = upsampfac;
+    RefPlan12Base* p = nullptr;
+    if (is_float) {
+      if (dim == 1) p = new RefPlan12<float, 1>(opt, sign, M, loc, modes);
+      if (dim == 2) p = new RefPlan12<float, 2>(opt, sign, M, loc, modes);
+      if (dim == 3) p = new RefPlan12<float, 3>(opt, sign, M, loc, modes);
+    } else {
+      if (dim == 1) p = new RefPlan12<double, 1>(opt, sign, M, loc, modes);
+      if (dim == 2) p = new RefPlan12<double, 2>(opt, sign, M, loc, modes);
+      if (dim == 3) p = new RefPlan12<double, 3>(opt, sign, M, loc, modes);
+    }
+    *handle = p;
+    return 0;
+  } catch (...) {
+    return code_of(std::current_exception());
+  }
+}
+
+__attribute__((visibility("default"))) int ref_plan12_set_points(void* h, int64_t M,
+                                                                 const void* const* loc) {
+  try {
+    static_cast<RefPlan12Base*>(h)->set_points(M, loc);
+    return 0;
+  } catch (...) {
+    return code_of(std::current_exception());
+  }
+}
+
+__attribute__((visibility("default"))) int ref_plan12_t1(void* h, const void* in, void* out,
+                                                         const int64_t* strides) {
+  try {
+    static_cast<RefPlan12Base*>(h)->t1(in, out, strides);
+    return 0;
+  } catch (...) {
+    return code_of(std::current_exception());
+  }
+}
+
+__attribute__((visibility("default"))) int ref_plan12_t2(void* h, const void* in,
+                                                         const int64_t* strides, void* out) {
+  try {
+    static_cast<RefPlan12Base*>(h)->t2(in, strides, out);
+    return 0;
+  } catch (...) {
+    return code_of(std::current_exception());
+  }
+}
+
+__attribute__((visibility("default"))) void ref_plan12_destroy(void* h) {
+  delete static_cast<RefPlan12Base*>(h);
 }
 
 __attribute__((visibility("default"))) int ref_gpu_type3(int is_float, int dim, double tol,
