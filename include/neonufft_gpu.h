@@ -233,6 +233,21 @@ NNB_API NeonufftError nnb_direct_type3_f64(int dim, int sign, int64_t num_in, co
                                    int64_t num_samples, const int64_t* target_idx, double* out,
                                    void* stream);
 
+/* Allocation-free FP64 direct type-1 sum (engine extension; it has no counterpart in the
+ * reference). Same arguments and results as nnb_direct_type1_f64, for callers that cannot call
+ * cudaMalloc (a caller-owned memory pool holding the whole device, or code that must not
+ * allocate after start-up): the per-block partial sums go to a fixed 16 MiB scratch array in
+ * the library's own device memory, kept on every GPU that loads the library until exit, and are
+ * added in a fixed order, so the result is also bit-reproducible. Limit:
+ * num_samples * ceil(num_nu / 4096) <= 1048576, else NEONUFFT_INPUT_ERROR. Nothing is
+ * allocated; the first call on a device looks up the scratch address (make it before any
+ * stream capture). All calls share the scratch: calls that overlap on the GPU race. */
+NNB_API NeonufftError nnb_direct_type1_f64_noalloc(int dim, int sign, int64_t num_nu,
+                                                   const double* const* loc, const double* in,
+                                                   int64_t num_samples,
+                                                   const int64_t* modes_idx, double* out,
+                                                   void* stream);
+
 /* Host-only parameter queries (engine extensions; no GPU needed). They expose the engine's own
  * restatement of the reference's heuristics so that sizing can be planned ahead:
  *  - ES kernel width w, shape beta and c = 4/w^2 as used by a plan of this precision

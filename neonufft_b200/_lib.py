@@ -81,6 +81,7 @@ SIGNATURES = [
     ("nnb_plan_t3_enable_timing", _E, [_P, C.c_int]),
     ("nnb_plan_t3_stage_times", _E, [_P, _PD, _PI64, C.c_int]),
     ("nnb_direct_type1_f64", _E, [C.c_int, C.c_int, _I64, _PP, _P, _I64, _P, _P, _P]),
+    ("nnb_direct_type1_f64_noalloc", _E, [C.c_int, C.c_int, _I64, _PP, _P, _I64, _P, _P, _P]),
     ("nnb_direct_type2_f64", _E, [C.c_int, C.c_int, _PI64, _P, _PP, _I64, _P, _P, _P]),
     ("nnb_direct_type3_f64", _E, [C.c_int, C.c_int, _I64, _PP, _P, _PP, _I64, _P, _P, _P]),
     ("nnb_es_kernel_params", _E, [C.c_double, C.c_double, C.c_int, C.POINTER(C.c_int), _PD, _PD]),

@@ -345,6 +345,24 @@ NeonufftError nnb_direct_type1_f64(int dim, int sign, int64_t num_nu, const doub
   });
 }
 
+NeonufftError nnb_direct_type1_f64_noalloc(int dim, int sign, int64_t num_nu,
+                                           const double* const* loc, const double* in,
+                                           int64_t num_samples, const int64_t* modes_idx,
+                                           double* out, void* stream) {
+  return guard([&] {
+    if (dim < 1 || dim > 3) nnb::throw_input("dimension must be 1, 2 or 3");
+    if (num_nu < 0 || num_samples < 0) nnb::throw_input("negative size");
+    need(out, "output");
+    if (num_samples > 0) need(modes_idx, "mode indices");
+    if (num_nu > 0) {
+      need(loc, "coordinates");
+      need(in, "input");
+    }
+    nnb::launch_direct_type1_noalloc(dim, sign < 0 ? -1 : 1, num_nu, loc, in, num_samples,
+                                     modes_idx, out, static_cast<cudaStream_t>(stream));
+  });
+}
+
 NeonufftError nnb_direct_type2_f64(int dim, int sign, const int64_t* n_modes, const double* in,
                                    const double* const* loc, int64_t num_samples,
                                    const int64_t* point_idx, double* out, void* stream) {

@@ -111,5 +111,9 @@ void launch_direct_type2(int dim, int sign, const i64* n_modes, const double* in
 void launch_direct_type3(int dim, int sign, i64 M, const double* const* in_loc, const double* in,
                          const double* const* out_loc, i64 S, const i64* target_idx,
                          double* out, cudaStream_t stream);
+// Same sums as launch_direct_type1 through a fixed device scratch array (direct_noalloc.cu).
+void launch_direct_type1_noalloc(int dim, int sign, i64 M, const double* const* loc,
+                                 const double* in, i64 S, const i64* modes_idx, double* out,
+                                 cudaStream_t stream);
 
 }  // namespace nnb
