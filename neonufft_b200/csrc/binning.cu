@@ -43,18 +43,16 @@ __global__ void __launch_bounds__(kBinBlock)
     bin_count_kernel(BinGeom g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks, int* err) {
   for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
        i += i64(gridDim.x) * kBinBlock) {
-    i64 tile_lin = 0;
-    i64 mul = 1;
+    i64 t[3] = {0, 0, 0};
     bool ok = true;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-      i64 i0;
+      i64 i0 = 0;
       double frac;
       ok &= cell_of(g, d, double(x.p[d][i]), i0, frac);
-      if (!ok) i0 = 0;
-      tile_lin += (i0 / g.tile[d]) * mul;
-      mul *= g.ntiles[d];
+      t[d] = i0 / g.tile[d];
     }
+    i64 tile_lin = tile_linear(g, t);
     if (!ok) {
       atomicOr(err, 1);
       tile_lin = 0;
@@ -69,8 +67,7 @@ __global__ void __launch_bounds__(kBinBlock)
                        u32* perm, u32* local, T* f0, T* f1, T* f2) {
   for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
        i += i64(gridDim.x) * kBinBlock) {
-    i64 tile_lin = 0;
-    i64 mul = 1;
+    i64 t[3] = {0, 0, 0};
     int l[3] = {0, 0, 0};
     double fr[3] = {0, 0, 0};
     i64 i0[3] = {0, 0, 0};
@@ -85,11 +82,10 @@ __global__ void __launch_bounds__(kBinBlock)
         i0[d] = 0;
         fr[d] = -0.5 * g.w;
       }
-      const i64 t = i0[d] / g.tile[d];
-      l[d] = int(i0[d] - t * g.tile[d]);
-      tile_lin += t * mul;
-      mul *= g.ntiles[d];
+      t[d] = i0[d] / g.tile[d];
+      l[d] = int(i0[d] - t[d] * g.tile[d]);
     }
+    const i64 tile_lin = tile_linear(g, t);
     const u32 pos = bin_start[tile_lin] + ranks[i];
     perm[pos] = u32(i);
     local[pos] = pack_local(DIM, l[0], l[1], l[2]);

@@ -90,7 +90,19 @@ struct BinGeom {
   i64 total_tiles;
   double offset[3];   // affine pre-transform (type 3); 0 / 1 otherwise
   double scale[3];
+  int zmajor;         // 3D: bins ordered plane-fastest, tz + ntz (tx + ntx ty); else x-fastest
 };
+
+// Linear bin index of tile coordinates t[0..dim).
+__host__ __device__ __forceinline__ i64 tile_linear(const BinGeom& g, const i64* t) {
+  if (g.dim == 3 && g.zmajor) return t[2] + i64(g.ntiles[2]) * (t[0] + i64(g.ntiles[0]) * t[1]);
+  i64 lin = 0, mul = 1;
+  for (int d = 0; d < g.dim; ++d) {
+    lin += t[d] * mul;
+    mul *= g.ntiles[d];
+  }
+  return lin;
+}
 
 // Packed tile-local start cell of a point: 1D 32 bits; 2D 16+16; 3D 11+11+10 (x, y, z).
 __host__ __device__ __forceinline__ u32 pack_local(int dim, int lx, int ly, int lz) {

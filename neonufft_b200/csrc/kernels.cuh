@@ -38,10 +38,12 @@ struct SpreadArgs {
   int batch;
   T beta;
   T c;
-  int method;  // 1: warp per point, 2: thread per point
+  int method;  // 1: warp-private slabs, 2: thread per point, 3: z-window (zwin.cu)
 };
 template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream);
+template <typename T>
+void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream);
 // Dynamic shared memory of the default spreading / interpolation kernels for a tile shape.
 size_t spread_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
 size_t interp_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
@@ -56,10 +58,12 @@ struct InterpArgs {
   cplx_t<T>* out;              // original point order
   T beta;
   T c;
-  int method;  // 1: warp per point, 2: thread per point
+  int method;  // 1: warp per point, 2: thread per point, 3: z-window (zwin.cu)
 };
 template <typename T>
 void launch_interp(const InterpArgs<T>& a, cudaStream_t stream);
+template <typename T>
+void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream);
 
 // ---- deconvolution (deconv.cu) --------------------------------------------------------------
 template <typename T>

@@ -9,7 +9,7 @@ namespace nnb {
 
 namespace {
 
-// Default spreading / interpolation method (see spread.cu and interp.cu).
+// Placeholder until the constructor resolves the method (choose_method in runtime.cu).
 constexpr int kDefaultMethod = 1;
 
 template <typename T>
@@ -58,7 +58,7 @@ void validate_options(const NnbOptions& opt) {
   for (int d = 0; d < 3; ++d) {
     if (opt.tile[d] < 0) throw_input("invalid tile shape");
   }
-  if (opt.spread_method < 0 || opt.spread_method > 2) throw_input("invalid spread method");
+  if (opt.spread_method < 0 || opt.spread_method > 3) throw_input("invalid spread method");
   if (opt.n_spread != 0 && (opt.n_spread < 2 || opt.n_spread > 16)) {
     throw_input("kernel width must be in [2, 16]");
   }
@@ -89,15 +89,15 @@ public:
     }
     kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
-    if (opt.spread_method > 0) method_ = opt.spread_method;
+    method_ = choose_method(dim, kp_.w, opt.spread_method);
     for (int d = 0; d < dim; ++d) nf_[d] = fine_grid_size(modes_[d], opt.upsampfac, kp_.w);
     fft_ = std::make_unique<FftGrid<T>>(alloc_, dim, nf_, sign_, stream_);
     for (int d = 0; d < dim; ++d) {
       corr_[d].set_allocator(alloc_);
       upload(corr_[d], deconv_factors(kp_, nf_[d]), stream_);
     }
-    choose_tile(dim, kp_.w, sizeof(cplx_t<T>), nf_, opt.tile, tile_);
-    geom_ = make_geom(dim, kp_.w, nf_, tile_, nullptr, nullptr);
+    choose_tile(dim, kp_.w, sizeof(cplx_t<T>), nf_, opt.tile, method_, tile_);
+    geom_ = make_geom(dim, kp_.w, nf_, tile_, nullptr, nullptr, method_ == 3);
     set_points(M, loc);
   }
 
@@ -247,7 +247,7 @@ public:
     if (batch > 65535) throw_input("batch size above 65535");
     kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
-    if (opt.spread_method > 0) method_ = opt.spread_method;
+    method_ = choose_method(dim, kp_.w, opt.spread_method);
     for (auto& c : corr_) c.set_allocator(alloc_);
   }
 
@@ -330,8 +330,8 @@ public:
       quad_.z[i] = quad.z[i];
       quad_.kv[i] = quad.kv[i];
     }
-    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nf1_, opt_.tile, in_tile_);
-    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nfft_, opt_.tile, out_tile_);
+    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nf1_, opt_.tile, method_, in_tile_);
+    choose_tile(dim_, kp_.w, sizeof(cplx_t<T>), nfft_, opt_.tile, method_, out_tile_);
     NNB_CUDA(cudaStreamSynchronize(stream_));
   }
 
@@ -352,7 +352,7 @@ public:
     }
     double scale[3];
     for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? 1.0 / gamma_[d] : 1.0;
-    const BinGeom g = make_geom(dim_, kp_.w, nf1_, in_tile_, C_, scale);
+    const BinGeom g = make_geom(dim_, kp_.w, nf1_, in_tile_, C_, scale, method_ == 3);
     ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
     in_points_.build(g, x, M, stream_);
   }
@@ -363,7 +363,7 @@ public:
     const CoordPtrs<T> s = coords<T>(dim_, pts);
     double scale[3];
     for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? gamma_[d] * h_[d] : 1.0;
-    const BinGeom g = make_geom(dim_, kp_.w, nfft_, out_tile_, D_, scale);
+    const BinGeom g = make_geom(dim_, kp_.w, nfft_, out_tile_, D_, scale, method_ == 3);
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
       out_points_.build(g, s, K, stream_);

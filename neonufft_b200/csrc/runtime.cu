@@ -253,11 +253,32 @@ template class PointSet<float>;
 template class PointSet<double>;
 
 // ---- tiles ----------------------------------------------------------------------------------------
+int choose_method(int dim, int w, int requested) {
+  if (requested == 3 && (dim != 3 || w > 8)) {
+    throw_input("spread method 3 needs a 3D plan with kernel width <= 8");
+  }
+  if (requested > 0) return requested;
+  return (dim == 3 && w <= 8) ? 3 : 1;
+}
+
 void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int* requested,
-                 int* tile) {
+                 int method, int* tile) {
   const int max_bits[3] = {dim == 3 ? 11 : (dim == 2 ? 16 : 31), dim == 3 ? 11 : 16, 10};
   bool explicit_tile = requested && requested[0] > 0;
   for (int d = 0; d < 3; ++d) tile[d] = 1;
+  if (method == 3) {
+    // x tile of 8 cells for single precision (15-cell register rows at w = 8), 4 for double.
+    tile[0] = complex_bytes == 8 ? 8 : 4;
+    if (explicit_tile) {
+      if (requested[0] != 4 && requested[0] != 8) {
+        throw_input("spread method 3 supports tiles of 4 or 8 cells in x");
+      }
+      tile[0] = requested[0];
+    }
+    tile[1] = 8;
+    tile[2] = 1;
+    return;
+  }
   if (explicit_tile) {
     for (int d = 0; d < dim; ++d) {
       const int t = requested[d];
@@ -307,10 +328,11 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
 }
 
 BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* offset,
-                  const double* scale) {
+                  const double* scale, int zmajor) {
   BinGeom g{};
   g.dim = dim;
   g.w = w;
+  g.zmajor = (dim == 3 && zmajor) ? 1 : 0;
   g.total_tiles = 1;
   for (int d = 0; d < 3; ++d) {
     if (d < dim) {

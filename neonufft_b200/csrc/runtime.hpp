@@ -150,11 +150,17 @@ private:
   DevArray<int> err_;
 };
 
-// Tile shape for a grid: explicit request (validated) or the automatic choice.
-void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int* requested,
-                 int* tile);
+// Spreading / interpolation method for a plan: the requested one (validated), or the default:
+// 3 (z-window, zwin.cu) for 3D plans with n_spread <= 8, else 1 (shared-memory slabs).
+int choose_method(int dim, int w, int requested);
 
+// Tile shape for a grid and method: explicit request (validated) or the automatic choice.
+// Method 3 uses (tx, 8, 1) tiles, tx in {4, 8}.
+void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int* requested,
+                 int method, int* tile);
+
+// zmajor: order the bins plane-fastest (method 3).
 BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* offset,
-                  const double* scale);
+                  const double* scale, int zmajor = 0);
 
 }  // namespace nnb
