@@ -9,7 +9,8 @@
 //    i0 - loc, so single-precision plans keep the full double-precision position;
 //  - pass 1 records each point's rank inside its tile (the only atomic);
 //  - a three-kernel device-wide exclusive scan gives tile offsets in tile order;
-//  - pass 2 writes structure-of-arrays records (perm, local, frac[d]) with no atomics.
+//  - pass 2 writes one 32-byte record per point (perm, packed cell, fractions), a full sector,
+//    with no atomics.
 #include "kernels.cuh"
 
 namespace nnb {
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(kBinBlock)
 template <typename T, int DIM>
 __global__ void __launch_bounds__(kBinBlock)
     bin_scatter_kernel(BinGeom g, CoordPtrs<T> x, i64 M, const u32* ranks, const u32* bin_start,
-                       u32* perm, u32* local, T* f0, T* f1, T* f2) {
+                       PointRec<T>* recs) {
   for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
        i += i64(gridDim.x) * kBinBlock) {
     i64 t[3] = {0, 0, 0};
@@ -87,11 +88,13 @@ __global__ void __launch_bounds__(kBinBlock)
     }
     const i64 tile_lin = tile_linear(g, t);
     const u32 pos = bin_start[tile_lin] + ranks[i];
-    perm[pos] = u32(i);
-    local[pos] = pack_local(DIM, l[0], l[1], l[2]);
-    f0[pos] = T(fr[0]);
-    if (DIM > 1) f1[pos] = T(fr[1]);
-    if (DIM > 2) f2[pos] = T(fr[2]);
+    PointRec<T> r;
+    r.perm = u32(i);
+    r.local = pack_local(DIM, l[0], l[1], l[2]);
+    r.frac[0] = T(fr[0]);
+    r.frac[1] = T(fr[1]);
+    r.frac[2] = T(fr[2]);
+    recs[pos] = r;
   }
 }
 
@@ -225,24 +228,22 @@ void launch_exclusive_scan(const u32* counts, u32* out, i64 n, u32* tmp, cudaStr
   NNB_LAUNCH_CHECK();
 }
 
-template <typename T, typename TF>
+template <typename T>
 void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
-                        const u32* bin_start, u32* perm, u32* local, TF* f0, TF* f1, TF* f2,
-                        cudaStream_t stream) {
-  static_assert(std::is_same<T, TF>::value, "fractions are stored in the plan precision");
+                        const u32* bin_start, PointRec<T>* rec, cudaStream_t stream) {
   if (M <= 0) return;
   const int grid = grid_for(M, kBinBlock);
   switch (g.dim) {
-    case 1: bin_scatter_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
-    case 2: bin_scatter_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
-    default: bin_scatter_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, perm, local, f0, f1, f2); break;
+    case 1: bin_scatter_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
+    case 2: bin_scatter_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
+    default: bin_scatter_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
   }
   NNB_LAUNCH_CHECK();
 }
 
 template void launch_bin_count<float>(const BinGeom&, CoordPtrs<float>, i64, u32*, u32*, int*, cudaStream_t);
 template void launch_bin_count<double>(const BinGeom&, CoordPtrs<double>, i64, u32*, u32*, int*, cudaStream_t);
-template void launch_bin_scatter<float, float>(const BinGeom&, CoordPtrs<float>, i64, const u32*, const u32*, u32*, u32*, float*, float*, float*, cudaStream_t);
-template void launch_bin_scatter<double, double>(const BinGeom&, CoordPtrs<double>, i64, const u32*, const u32*, u32*, u32*, double*, double*, double*, cudaStream_t);
+template void launch_bin_scatter<float>(const BinGeom&, CoordPtrs<float>, i64, const u32*, const u32*, PointRec<float>*, cudaStream_t);
+template void launch_bin_scatter<double>(const BinGeom&, CoordPtrs<double>, i64, const u32*, const u32*, PointRec<double>*, cudaStream_t);
 
 }  // namespace nnb

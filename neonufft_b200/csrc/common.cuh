@@ -121,13 +121,23 @@ __host__ __device__ __forceinline__ void unpack_local(int dim, u32 v, int& lx, i
 }
 constexpr int kMaxTileBits3[3] = {11, 11, 10};
 
-// Device-side view of a bin-sorted point set (structure of arrays, length M, sorted by tile).
+// One bin-sorted point: 32 bytes (a full 32-byte sector) for float and double plans, so that
+// the binning scatter writes each point with one sector and the kernels read it with two
+// 16-byte loads.
+template <typename T>
+struct alignas(16) PointRec {
+  u32 perm;   // original point index
+  u32 local;  // packed tile-local start cell
+  T frac[3];  // kernel argument of the first cell, i0 - loc, in [-w/2, -w/2 + 1]
+};
+static_assert(sizeof(PointRec<float>) == 32 && sizeof(PointRec<double>) == 32,
+              "point records are one 32-byte sector");
+
+// Device-side view of a bin-sorted point set (records in tile order, length M).
 template <typename T>
 struct SortedPoints {
-  const u32* perm;       // original point index
-  const u32* local;      // packed tile-local start cell
-  const T* frac[3];      // kernel argument of the first cell, i0 - loc, in [-w/2, -w/2 + 1]
-  const u32* bin_start;  // total_tiles + 1 offsets into the sorted arrays
+  const PointRec<T>* rec;
+  const u32* bin_start;  // total_tiles + 1 offsets into the records
 };
 
 // ES kernel (exponential of semicircle): phi(x) = exp(beta * (sqrt(1 - c x^2) - 1)) for

@@ -129,16 +129,16 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
     u32 my_idx = 0;
     C my_post{T(1), T(0)};
     if (lane < nb) {
-      const u32 p = b + lane;
-      my_idx = a.pts.perm[p];
+      const PointRec<T> rec = a.pts.rec[b + lane];
+      my_idx = rec.perm;
       if (a.postphase) my_post = a.postphase[my_idx];
       int lx, ly, lz;
-      unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+      unpack_local(DIM, rec.local, lx, ly, lz);
       my_base = shift + lz * L.PS + ly * L.RS + lx;
       T* kr = kvb + lane * KS;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
-        const T f = a.pts.frac[d][p];
+        const T f = rec.frac[d];
 #pragma unroll
         for (int k = 0; k < W; ++k) kr[d * W + k] = es_eval_fast<T>(f + T(k), a.beta, a.c);
       }
@@ -218,17 +218,18 @@ __global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a
                        t1 * g.tile[1], t2 * g.tile[2], a.grid, tile);
   __syncthreads();
   for (u32 p = start + threadIdx.x; p < end; p += kTppThreads) {
+    const PointRec<T> rec = a.pts.rec[p];
     int lx, ly, lz;
-    unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+    unpack_local(DIM, rec.local, lx, ly, lz);
     T kx[W];
-    const T fx = a.pts.frac[0][p];
+    const T fx = rec.frac[0];
 #pragma unroll
     for (int k = 0; k < W; ++k) kx[k] = es_eval_fast<T>(fx + T(k), a.beta, a.c);
     T sx = 0, sy = 0;
     const int nz = DIM > 2 ? W : 1;
     const int ny = DIM > 1 ? W : 1;
-    const T fy = DIM > 1 ? a.pts.frac[1][p] : T(0);
-    const T fz = DIM > 2 ? a.pts.frac[2][p] : T(0);
+    const T fy = DIM > 1 ? rec.frac[1] : T(0);
+    const T fz = DIM > 2 ? rec.frac[2] : T(0);
 #pragma unroll 1
     for (int dz = 0; dz < nz; ++dz) {
       const T kz = DIM > 2 ? es_eval_fast<T>(fz + T(dz), a.beta, a.c) : T(1);
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a
         sy += ky * ry;
       }
     }
-    const u32 idx = a.pts.perm[p];
+    const u32 idx = rec.perm;
     C res{sx, sy};
     if (a.postphase) res = cmul(res, a.postphase[idx]);
     a.out[idx] = res;

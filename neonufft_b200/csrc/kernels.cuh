@@ -19,11 +19,10 @@ void launch_bin_count(const BinGeom& g, CoordPtrs<T> x, i64 M, u32* counts, u32*
 // Exclusive scan of n counts into out[0..n] (out[n] = total). tmp needs scan_tmp_words(n).
 i64 scan_tmp_words(i64 n);
 void launch_exclusive_scan(const u32* counts, u32* out, i64 n, u32* tmp, cudaStream_t stream);
-// Pass 2: permutation and packed per-point data in tile order.
-template <typename T, typename TF>
+// Pass 2: one 32-byte record per point (permutation, packed cell, fractions) in tile order.
+template <typename T>
 void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
-                        const u32* bin_start, u32* perm, u32* local, TF* frac0, TF* frac1,
-                        TF* frac2, cudaStream_t stream);
+                        const u32* bin_start, PointRec<T>* rec, cudaStream_t stream);
 
 // ---- spreading (spread.cu) ------------------------------------------------------------------
 template <typename T>

@@ -194,10 +194,8 @@ template class FftGrid<double>;
 // ---- point sets -------------------------------------------------------------------------------
 template <typename T>
 PointSet<T>::PointSet(std::shared_ptr<DeviceAllocator> alloc)
-    : perm_(alloc), local_(alloc), counts_(alloc), bin_start_(alloc), ranks_(alloc),
-      scan_tmp_(alloc), err_(alloc) {
-  for (auto& f : frac_) f.set_allocator(alloc);
-}
+    : rec_(alloc), counts_(alloc), bin_start_(alloc), ranks_(alloc), scan_tmp_(alloc),
+      err_(alloc) {}
 
 template <typename T>
 void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream) {
@@ -212,24 +210,14 @@ void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t st
   counts_.reserve(size_t(nt));
   bin_start_.reserve(size_t(nt + 1));
   scan_tmp_.reserve(size_t(scan_tmp_words(nt)));
-  perm_.reserve(size_t(M));
-  local_.reserve(size_t(M));
+  rec_.reserve(size_t(M));
   ranks_.reserve(size_t(M));
-  for (int d = 0; d < 3; ++d) {
-    if (d < g.dim) {
-      frac_[d].reserve(size_t(M));
-    } else {
-      frac_[d].release();
-    }
-  }
   err_.reserve(1);
   NNB_CUDA(cudaMemsetAsync(counts_.data(), 0, sizeof(u32) * nt, stream));
   NNB_CUDA(cudaMemsetAsync(err_.data(), 0, sizeof(int), stream));
   launch_bin_count<T>(g, x, M, counts_.data(), ranks_.data(), err_.data(), stream);
   launch_exclusive_scan(counts_.data(), bin_start_.data(), nt, scan_tmp_.data(), stream);
-  launch_bin_scatter<T, T>(g, x, M, ranks_.data(), bin_start_.data(), perm_.data(),
-                           local_.data(), frac_[0].data(), frac_[1].data(), frac_[2].data(),
-                           stream);
+  launch_bin_scatter<T>(g, x, M, ranks_.data(), bin_start_.data(), rec_.data(), stream);
   int host_err = 0;
   NNB_CUDA(cudaMemcpyAsync(&host_err, err_.data(), sizeof(int), cudaMemcpyDeviceToHost, stream));
   NNB_CUDA(cudaStreamSynchronize(stream));
@@ -242,9 +230,7 @@ void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t st
 template <typename T>
 SortedPoints<T> PointSet<T>::view() const {
   SortedPoints<T> v;
-  v.perm = perm_.data();
-  v.local = local_.data();
-  for (int d = 0; d < 3; ++d) v.frac[d] = frac_[d].data();
+  v.rec = rec_.data();
   v.bin_start = bin_start_.data();
   return v;
 }

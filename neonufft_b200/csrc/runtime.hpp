@@ -145,8 +145,8 @@ public:
 private:
   BinGeom g_{};
   i64 M_ = 0;
-  DevArray<u32> perm_, local_, counts_, bin_start_, ranks_, scan_tmp_;
-  DevArray<T> frac_[3];
+  DevArray<PointRec<T>> rec_;
+  DevArray<u32> counts_, bin_start_, ranks_, scan_tmp_;
   DevArray<int> err_;
 };
 

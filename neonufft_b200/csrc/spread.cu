@@ -144,17 +144,17 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
       int my_base = 0;
       C my_v{T(0), T(0)};
       if (lane < nb) {
-        const u32 p = b + lane;
-        const u32 idx = a.pts.perm[p];
+        const PointRec<T> rec = a.pts.rec[b + lane];
+        const u32 idx = rec.perm;
         my_v = in[idx];
         if (a.prephase) my_v = cmul(my_v, a.prephase[idx]);
         int lx, ly, lz;
-        unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+        unpack_local(DIM, rec.local, lx, ly, lz);
         my_base = lz * L.PS + ly * L.RS + lx;
         T* kr = kvb + lane * KS;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const T f = a.pts.frac[d][p];
+          const T f = rec.frac[d];
 #pragma unroll
           for (int k = 0; k < W; ++k) kr[d * W + k] = es_eval_fast<T>(f + T(k), a.beta, a.c);
         }
@@ -312,17 +312,18 @@ __global__ void __launch_bounds__(kTppThreads) spread_tpp_kernel(SpreadArgs<T> a
   __syncthreads();
 
   for (u32 p = start + threadIdx.x; p < end; p += kTppThreads) {
-    const u32 idx = a.pts.perm[p];
+    const PointRec<T> rec = a.pts.rec[p];
+    const u32 idx = rec.perm;
     C v = in[idx];
     if (a.prephase) v = cmul(v, a.prephase[idx]);
     int lx, ly, lz;
-    unpack_local(DIM, a.pts.local[p], lx, ly, lz);
+    unpack_local(DIM, rec.local, lx, ly, lz);
     T kx[W];
-    const T fx = a.pts.frac[0][p];
+    const T fx = rec.frac[0];
 #pragma unroll
     for (int k = 0; k < W; ++k) kx[k] = es_eval_fast<T>(fx + T(k), a.beta, a.c);
-    const T fy = DIM > 1 ? a.pts.frac[1][p] : T(0);
-    const T fz = DIM > 2 ? a.pts.frac[2][p] : T(0);
+    const T fy = DIM > 1 ? rec.frac[1] : T(0);
+    const T fz = DIM > 2 ? rec.frac[2] : T(0);
     const int nz = DIM > 2 ? W : 1;
     const int ny = DIM > 1 ? W : 1;
 #pragma unroll 1

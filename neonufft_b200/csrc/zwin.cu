@@ -8,52 +8,54 @@
 // Points are binned by (x tile of TX cells, y tile of 8 cells, single z plane), and the bins of
 // one (x, y) column are consecutive in plane order (BinGeom::zmajor). One CTA walks one column
 // over a chunk of planes. Its region is P0 x P1 cells in (x, y), P0 = TX + w - 1 and
-// P1 = 8 + w - 1, and RZ >= w consecutive planes in z:
-//  * thread (a, b), a = y residue mod 8, b = z residue mod RZ, keeps in registers the region
-//    rows y = a, a + 8 (all P0 cells of each) of the one plane p = b (mod RZ) that lies in the
-//    current window [t, t + RZ). Each point whose footprint starts at plane t touches, for
-//    w = 8, exactly one of those rows in every thread: no two threads share a cell, so there
-//    are no atomics and no shared-memory traffic per cell;
-//  * the points of plane t are staged once in shared memory (one thread per point: its kernel
-//    values placed over the region's x range, zero elsewhere, so that every thread applies
-//    them with fixed register indices; strength times ky; kz; y offset);
-//  * every thread then adds c * kx[i] * ky * kz to its row cells with packed two-float FMAs
-//    (fma.rn.f32x2 on sm_100a), the complex strength being the packed pair;
-//  * spreading: after plane t the plane is complete, and the threads holding it add it to the
-//    fine grid (float2 / double2 atomics: neighbouring columns and chunks overlap by the halo)
-//    and start on plane t + RZ;
+// P1 = 8 + w - 1 <= 15, times a window of RZ >= w consecutive planes:
+//  * thread (a, b) keeps in registers the whole region row y = a (P0 cells, as pairs of
+//    neighbouring cells) of the one window plane p = b (mod RZ). The 16 rows a are split over
+//    the warps, LA = 32 / RZ rows per warp, so for a point whose footprint covers rows
+//    [ly, ly + w) a warp either owns some of them or skips the point with a warp-uniform
+//    branch; no thread holds a cell that another thread updates, so there are no atomics and
+//    no shared-memory traffic per cell;
+//  * the points of plane t are staged in shared memory (one thread per point): kx over the
+//    region's x range, strength * ky over the 16 rows and kz over the RZ planes, each zero
+//    outside the footprint, so that every thread applies them with fixed register indices and
+//    no range tests;
+//  * each owning thread updates its row with packed two-float FMAs (fma.rn.f32x2 on sm_100a),
+//    one for the real and one for the imaginary parts of two neighbouring cells;
+//  * spreading: when plane t is complete, the threads holding it add it to the fine grid
+//    (float2 / double2 atomics: neighbouring columns and chunks overlap by the halo) and start
+//    on plane t + RZ;
 //  * interpolation: the threads holding plane t reload their rows with plane t + RZ, fetched
-//    with cp.async while plane t's points are processed; per point the row sums of all threads
-//    are reduced over the warp for eight points at a time (transposed butterfly), then over
-//    the CTA's warps through shared memory.
+//    with cp.async while plane t's points are processed; per point the row sums are reduced
+//    for eight points at a time through a per-warp shared-memory transpose, then over warps.
 #include "kernels.cuh"
 
 namespace nnb {
 
 namespace {
 
-// ---- packed complex arithmetic ---------------------------------------------------------------
+// ---- packed arithmetic on pairs of values --------------------------------------------------------
 template <typename T>
 struct Packed;
 
 template <>
 struct Packed<float> {
-  using P = unsigned long long;  // (re, im) in one 64-bit register pair
+  using P = unsigned long long;  // two floats in one 64-bit register pair
   static __device__ __forceinline__ P zero() { return 0ull; }
   static __device__ __forceinline__ P pack(float x, float y) {
     P r;
     asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
     return r;
   }
-  static __device__ __forceinline__ P splat(float x) {
-    P r;
-    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(x));
-    return r;
+  static __device__ __forceinline__ P splat(float x) { return pack(x, x); }
+  static __device__ __forceinline__ float lo(P v) {
+    float x, y;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+    return x;
   }
-  static __device__ __forceinline__ float2 unpack(P v) {
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-    return r;
+  static __device__ __forceinline__ float hi(P v) {
+    float x, y;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+    return y;
   }
   // a * b + c, elementwise
   static __device__ __forceinline__ P fma(P a, P b, P c) {
@@ -61,18 +63,10 @@ struct Packed<float> {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
   }
-  static __device__ __forceinline__ P mul(P a, P b) {
-    P d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-  }
   static __device__ __forceinline__ P add(P a, P b) {
     P d;
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
-  }
-  static __device__ __forceinline__ P shfl_xor(P v, int m) {
-    return __shfl_xor_sync(0xffffffffu, v, m);
   }
 };
 
@@ -82,16 +76,28 @@ struct Packed<double> {
   static __device__ __forceinline__ P zero() { return P{0.0, 0.0}; }
   static __device__ __forceinline__ P pack(double x, double y) { return P{x, y}; }
   static __device__ __forceinline__ P splat(double x) { return P{x, x}; }
-  static __device__ __forceinline__ double2 unpack(P v) { return v; }
+  static __device__ __forceinline__ double lo(P v) { return v.x; }
+  static __device__ __forceinline__ double hi(P v) { return v.y; }
   static __device__ __forceinline__ P fma(P a, P b, P c) {
     return P{::fma(a.x, b.x, c.x), ::fma(a.y, b.y, c.y)};
   }
-  static __device__ __forceinline__ P mul(P a, P b) { return P{a.x * b.x, a.y * b.y}; }
   static __device__ __forceinline__ P add(P a, P b) { return P{a.x + b.x, a.y + b.y}; }
-  static __device__ __forceinline__ P shfl_xor(P v, int m) {
-    return P{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
-  }
 };
+
+// Four consecutive values of a 16-byte aligned shared-memory array as two pairs.
+template <typename T>
+__device__ __forceinline__ void load_pairs(const T* p, typename Packed<T>::P* k);
+template <>
+__device__ __forceinline__ void load_pairs<float>(const float* p, unsigned long long* k) {
+  const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+  k[0] = v.x;
+  k[1] = v.y;
+}
+template <>
+__device__ __forceinline__ void load_pairs<double>(const double* p, double2* k) {
+  k[0] = *reinterpret_cast<const double2*>(p);
+  k[1] = *reinterpret_cast<const double2*>(p + 2);
+}
 
 __device__ __forceinline__ void atomic_add_cplx(float2* p, float2 v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_cplx(double2* p, double2 v) {
@@ -102,178 +108,188 @@ __device__ __forceinline__ void atomic_add_cplx(double2* p, double2 v) {
 // ---- geometry ----------------------------------------------------------------------------------
 template <int W, int TX>
 struct ZShape {
-  static constexpr int RY = 8;                   // y residues (threads per z residue)
-  static constexpr int RZ = W <= 4 ? 4 : 8;      // z residues = window planes (>= W)
-  static constexpr int NT = RY * RZ;             // threads per CTA
-  static constexpr int TY = 8;                   // tile y
-  static constexpr int P0 = TX + W - 1;          // region x extent
-  static constexpr int P0R = (P0 + 1) & ~1;      // padded to an even count (16-byte loads)
-  static constexpr int P1 = TY + W - 1;          // region y extent
-  static constexpr int NYR = (P1 + RY - 1) / RY; // region rows per thread
-  static_assert(W <= RZ, "window narrower than the kernel");
+  static constexpr int RZ = W <= 4 ? 4 : 8;   // window planes = z residues (>= W)
+  static constexpr int LA = 32 / RZ;          // rows per warp
+  static constexpr int RY = 16;               // region rows (>= P1)
+  static constexpr int NWARP = RY / LA;
+  static constexpr int NT = 32 * NWARP;       // threads per CTA
+  static constexpr int TY = 8;                // tile y
+  static constexpr int P0 = TX + W - 1;       // region x extent (cells)
+  static constexpr int NP = (P0 + 1) / 2;     // cell pairs per row
+  static constexpr int KXN = 4 * ((NP + 1) / 2);  // staged kx values (16-byte multiple)
+  static constexpr int P1 = TY + W - 1;       // region y extent
+  static constexpr int BATCH = 64;            // points staged at a time
+  static constexpr int G = 8;                 // points reduced together (interpolation)
+  static_assert(W <= RZ && P1 <= RY, "window smaller than the kernel footprint");
 };
 
 // Per-point data staged in shared memory (one slot per point of a batch).
-template <typename T, int W, int P0R>
+template <typename T, int W, int TX, bool SPREAD>
 struct alignas(16) ZSlot {
-  typename Packed<T>::P kx[P0R];  // (k, k) over the region's x range, zero outside the footprint
-  typename Packed<T>::P kyv[W];   // spreading: strength * ky[d]; interpolation: (ky, ky)
-  T kz[W];
-  int ly;                         // first footprint row, tile-local
+  using S = ZShape<W, TX>;
+  using KY = typename std::conditional<SPREAD, cplx_t<T>, T>::type;
+  T kx[S::KXN];     // kx over the region's x range, zero outside the footprint
+  KY ky[S::RY];     // spreading: strength * ky per region row; interpolation: ky
+  T kz[S::RZ];      // kz per window offset, zero beyond w
+  int ly;           // first footprint row
 };
 
-// Stages point p (bin-sorted index) into slot `sl`; v is its strength (spreading only).
+// Stages bin-sorted point p into slot `sl`; v is its strength (spreading only).
 template <typename T, int W, int TX, bool SPREAD>
-__device__ __forceinline__ void stage_point(ZSlot<T, W, ZShape<W, TX>::P0R>& sl,
-                                            const SortedPoints<T>& pts, u32 p,
+__device__ __forceinline__ void stage_point(ZSlot<T, W, TX, SPREAD>& sl, const PointRec<T>& rec,
                                             cplx_t<T> v, T beta, T c) {
   using S = ZShape<W, TX>;
-  using Ops = Packed<T>;
-  const u32 loc = pts.local[p];
-  const int lx = int(loc & 0x7FFu);
-  const int ly = int((loc >> 11) & 0x7FFu);
-  const T fx = pts.frac[0][p];
-  const T fy = pts.frac[1][p];
-  const T fz = pts.frac[2][p];
+  const int lx = int(rec.local & 0x7FFu);
+  const int ly = int((rec.local >> 11) & 0x7FFu);
 #pragma unroll
-  for (int i = 0; i < S::P0R; ++i) sl.kx[i] = Ops::zero();
+  for (int i = 0; i < S::KXN; ++i) sl.kx[i] = T(0);
 #pragma unroll
-  for (int k = 0; k < W; ++k) sl.kx[lx + k] = Ops::splat(es_eval_fast<T>(fx + T(k), beta, c));
+  for (int i = 0; i < S::RY; ++i) {
+    if constexpr (SPREAD) {
+      sl.ky[i] = cplx_t<T>{T(0), T(0)};
+    } else {
+      sl.ky[i] = T(0);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < W; ++k) sl.kx[lx + k] = es_eval_fast<T>(rec.frac[0] + T(k), beta, c);
 #pragma unroll
   for (int k = 0; k < W; ++k) {
-    const T ky = es_eval_fast<T>(fy + T(k), beta, c);
-    sl.kyv[k] = SPREAD ? Ops::pack(v.x * ky, v.y * ky) : Ops::splat(ky);
-    sl.kz[k] = es_eval_fast<T>(fz + T(k), beta, c);
+    const T ky = es_eval_fast<T>(rec.frac[1] + T(k), beta, c);
+    if constexpr (SPREAD) {
+      sl.ky[ly + k] = cplx_t<T>{v.x * ky, v.y * ky};
+    } else {
+      sl.ky[ly + k] = ky;
+    }
   }
+#pragma unroll
+  for (int k = 0; k < S::RZ; ++k) sl.kz[k] = k < W ? es_eval_fast<T>(rec.frac[2] + T(k), beta, c) : T(0);
   sl.ly = ly;
 }
 
 // Chunk of planes handled by one CTA.
 struct ZChunks {
-  int len;      // planes per chunk
-  int count;    // chunks per column
+  int len;    // planes per chunk
+  int count;  // chunks per column
 };
 
-template <typename T>
 __device__ __forceinline__ i64 wrap_add(i64 base, int off, i64 n) {
   i64 i = base + off;
   while (i >= n) i -= n;
   return i;
 }
 
+// CTA coordinates: column (tx, ty) and plane range [z0, z1); false if the chunk has no points.
+struct ZCta {
+  int tx, ty, z0, z1;
+  i64 col;
+};
+__device__ __forceinline__ bool zcta(const BinGeom& g, const u32* bin_start, ZChunks ch,
+                                     ZCta& c, const u32*& bs) {
+  const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
+  const int chunk = int(blockIdx.x / ncols);
+  c.col = blockIdx.x - i64(chunk) * ncols;
+  c.tx = int(c.col % g.ntiles[0]);
+  c.ty = int(c.col / g.ntiles[0]);
+  const int nz = g.ntiles[2];  // == nf[2]: single-plane tiles
+  c.z0 = chunk * ch.len;
+  c.z1 = min(c.z0 + ch.len, nz);
+  bs = bin_start + c.col * nz;
+  return c.z0 < c.z1 && bs[c.z0] != bs[c.z1];
+}
+
 // ---- spreading ---------------------------------------------------------------------------------
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<W, TX>::NT, sizeof(T) == 4 ? 8 : 5)
+__global__ void __launch_bounds__(ZShape<W, TX>::NT)
     spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch) {
   using S = ZShape<W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  __shared__ ZSlot<T, W, S::P0R> slots[S::NT];
+  using Slot = ZSlot<T, W, TX, true>;
+  __shared__ Slot slots[S::BATCH];
 
   const BinGeom& g = a.g;
+  ZCta cta;
+  const u32* bs;
+  if (!zcta(g, a.pts.bin_start, ch, cta, bs)) return;
   const int tid = threadIdx.x;
-  const int ra = tid & (S::RY - 1);
-  const int rb = tid / S::RY;
-  const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
-  const int chunk = int(blockIdx.x / ncols);
-  const i64 col = blockIdx.x - i64(chunk) * ncols;
-  const int tx = int(col % g.ntiles[0]);
-  const int ty = int(col / g.ntiles[0]);
-  const int nz = g.ntiles[2];  // == nf[2]: single-plane tiles
-  const int z0 = chunk * ch.len;
-  const int z1 = min(z0 + ch.len, nz);
-  const u32* bs = a.pts.bin_start + col * nz;
-  if (z0 >= z1 || bs[z0] == bs[z1]) return;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int ra = warp * S::LA + lane % S::LA;  // region row
+  const int rb = lane / S::LA;                  // z residue
+  const int a_lo = warp * S::LA;                // first row of this warp
 
   const int batch = blockIdx.y;
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
-  const i64 gx0 = i64(tx) * TX;
-  const i64 gy0 = i64(ty) * S::TY;
+  const i64 gx0 = i64(cta.tx) * TX;
+  const i64 row_y = ra < S::P1 ? wrap_add(i64(cta.ty) * S::TY, ra, nfy) : 0;
 
-  P acc[S::NYR][S::P0];
+  P are[S::NP], aim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1)
 #pragma unroll
-  for (int j = 0; j < S::NYR; ++j) {
-#pragma unroll
-    for (int i = 0; i < S::P0; ++i) acc[j][i] = Ops::zero();
-  }
+  for (int q = 0; q < S::NP; ++q) are[q] = aim[q] = Ops::zero();
 
-  // Adds this thread's rows of plane p (absolute, may exceed nfz) to the grid and clears them.
+  // Adds this thread's row of plane p (absolute, may exceed nfz) to the grid and clears it.
   auto flush = [&](i64 p) {
-    const i64 gz = p % nfz;
+    if (ra < S::P1) {
+      C* row = grid + ((p % nfz) * nfy + row_y) * nfx;
 #pragma unroll
-    for (int j = 0; j < S::NYR; ++j) {
-      const int y = ra + S::RY * j;
-      if (y < S::P1) {
-        const i64 row = (gz * nfy + wrap_add<T>(gy0, y, nfy)) * nfx;
-#pragma unroll
-        for (int i = 0; i < S::P0; ++i) {
-          const C v = Ops::unpack(acc[j][i]);
-          acc[j][i] = Ops::zero();
-          if (v.x != T(0) || v.y != T(0)) atomic_add_cplx(&grid[row + wrap_add<T>(gx0, i, nfx)], v);
+      for (int q = 0; q < S::NP; ++q) {
+        const C v0{Ops::lo(are[q]), Ops::lo(aim[q])};
+        const C v1{Ops::hi(are[q]), Ops::hi(aim[q])};
+        are[q] = aim[q] = Ops::zero();
+        if (v0.x != T(0) || v0.y != T(0)) atomic_add_cplx(&row[wrap_add(gx0, 2 * q, nfx)], v0);
+        if (2 * q + 1 < S::P0 && (v1.x != T(0) || v1.y != T(0))) {
+          atomic_add_cplx(&row[wrap_add(gx0, 2 * q + 1, nfx)], v1);
         }
       }
     }
   };
 
-  u32 e = bs[z0];
-  for (int t = z0; t < z1; ++t) {
+  u32 e = bs[cta.z0];
+  for (int t = cta.z0; t < cta.z1; ++t) {
     const u32 s = e;
     e = bs[t + 1];
-    const int dz = (rb - t) & (S::RZ - 1);  // this thread's plane within the footprint
-    for (u32 base = s; base < e; base += S::NT) {
-      const int nb = int(min(e - base, u32(S::NT)));
+    const int dz = (rb - t) & (S::RZ - 1);  // this thread's plane within the window
+    for (u32 base = s; base < e; base += S::BATCH) {
+      const int nb = int(min(e - base, u32(S::BATCH)));
       if (tid < nb) {
-        const u32 p = base + tid;
-        const u32 idx = a.pts.perm[p];
-        C v = in[idx];
-        if (a.prephase) v = cmul(v, a.prephase[idx]);
-        stage_point<T, W, TX, true>(slots[tid], a.pts, p, v, a.beta, a.c);
+        const PointRec<T> rec = a.pts.rec[base + tid];
+        C v = in[rec.perm];
+        if (a.prephase) v = cmul(v, a.prephase[rec.perm]);
+        stage_point<T, W, TX, true>(slots[tid], rec, v, a.beta, a.c);
       }
       __syncthreads();
-      if (dz < W) {
-        for (int j = 0; j < nb; ++j) {
-          const ZSlot<T, W, S::P0R>& sl = slots[j];
-          const P kz = Ops::splat(sl.kz[dz]);
-          const int ly = sl.ly;
-          P wy[S::NYR];
+      for (int j = 0; j < nb; ++j) {
+        const Slot& sl = slots[j];
+        const int ly = sl.ly;
+        if (ly < a_lo + S::LA && ly + W > a_lo) {  // warp-uniform: this warp owns footprint rows
+          const C kyv = sl.ky[ra];
+          const T kzv = sl.kz[dz];
+          const P wre = Ops::splat(kyv.x * kzv);
+          const P wim = Ops::splat(kyv.y * kzv);
 #pragma unroll
-          for (int r = 0; r < S::NYR; ++r) {
-            const int dy = ra + S::RY * r - ly;
-            const int dyc = dy < 0 ? 0 : (dy >= W ? W - 1 : dy);
-            const P kv = sl.kyv[dyc];
-            wy[r] = (dy >= 0 && dy < W) ? Ops::mul(kv, kz) : Ops::zero();
-          }
-          if (sizeof(T) == 4) {
+          for (int q = 0; q < S::NP; q += 2) {
+            P k[2];
+            load_pairs<T>(&sl.kx[2 * q], k);
 #pragma unroll
-            for (int i = 0; i < S::P0; i += 2) {
-              const ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(&sl.kx[i]);
-              const P k0 = reinterpret_cast<const P&>(kk.x);
-              const P k1 = reinterpret_cast<const P&>(kk.y);
-#pragma unroll
-              for (int r = 0; r < S::NYR; ++r) {
-                acc[r][i] = Ops::fma(k0, wy[r], acc[r][i]);
-                if (i + 1 < S::P0) acc[r][i + 1] = Ops::fma(k1, wy[r], acc[r][i + 1]);
+            for (int u = 0; u < 2; ++u) {
+              if (q + u < S::NP) {
+                are[q + u] = Ops::fma(k[u], wre, are[q + u]);
+                aim[q + u] = Ops::fma(k[u], wim, aim[q + u]);
               }
-            }
-          } else {
-#pragma unroll
-            for (int i = 0; i < S::P0; ++i) {
-              const P k0 = sl.kx[i];
-#pragma unroll
-              for (int r = 0; r < S::NYR; ++r) acc[r][i] = Ops::fma(k0, wy[r], acc[r][i]);
             }
           }
         }
       }
       __syncthreads();
     }
-    if (rb == (t & (S::RZ - 1))) flush(t);
+    if (dz == 0) flush(t);
   }
   // planes [z1, z1 + w - 1) still hold contributions of this chunk's last planes
-  flush(z1 + ((rb - z1) & (S::RZ - 1)));
+  flush(cta.z1 + ((rb - cta.z1) & (S::RZ - 1)));
 }
 
 // ---- interpolation -----------------------------------------------------------------------------
@@ -289,185 +305,148 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<W, TX>::NT, sizeof(T) == 4 ? 8 : 5)
+__global__ void __launch_bounds__(ZShape<W, TX>::NT)
     interp_zwin_kernel(InterpArgs<T> a, ZChunks ch) {
   using S = ZShape<W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  constexpr int NW = S::NT / 32;
-  constexpr int G = 8;  // points reduced together
-  __shared__ ZSlot<T, W, S::P0R> slots[S::NT];
-  __shared__ P res[NW][S::NT];
-  __shared__ C stage[S::RY][S::NYR][S::P0];
+  using Slot = ZSlot<T, W, TX, false>;
+  constexpr int G = S::G;
+  constexpr int RS = 33;  // odd row stride of the transpose buffer: conflict-free reads
+  __shared__ Slot slots[S::BATCH];
+  __shared__ C red[S::NWARP][G][RS];
+  __shared__ C res[S::NWARP][S::BATCH];
+  __shared__ C stage[S::RY][2 * S::NP];
 
   const BinGeom& g = a.g;
+  ZCta cta;
+  const u32* bs;
+  if (!zcta(g, a.pts.bin_start, ch, cta, bs)) return;
   const int tid = threadIdx.x;
-  const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int ra = tid & (S::RY - 1);
-  const int rb = tid / S::RY;
-  const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
-  const int chunk = int(blockIdx.x / ncols);
-  const i64 col = blockIdx.x - i64(chunk) * ncols;
-  const int tx = int(col % g.ntiles[0]);
-  const int ty = int(col / g.ntiles[0]);
-  const int nz = g.ntiles[2];
-  const int z0 = chunk * ch.len;
-  const int z1 = min(z0 + ch.len, nz);
-  const u32* bs = a.pts.bin_start + col * nz;
-  if (z0 >= z1 || bs[z0] == bs[z1]) return;
+  const int lane = tid & 31;
+  const int ra = warp * S::LA + lane % S::LA;
+  const int rb = lane / S::LA;
+  const int a_lo = warp * S::LA;
+  const bool has_row = ra < S::P1;
 
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
-  const i64 gx0 = i64(tx) * TX;
-  const i64 gy0 = i64(ty) * S::TY;
-
-  // Row offsets (in cells) of this thread's region rows within a plane.
-  i64 rowoff[S::NYR];
-#pragma unroll
-  for (int j = 0; j < S::NYR; ++j) {
-    const int y = ra + S::RY * j;
-    rowoff[j] = y < S::P1 ? wrap_add<T>(gy0, y, nfy) * nfx : -1;
+  const i64 gx0 = i64(cta.tx) * TX;
+  const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, ra, nfy) : 0;
+  if (tid < S::RY) {
+    for (int i = S::P0; i < 2 * S::NP; ++i) stage[tid][i] = C{T(0), T(0)};  // padding cell
   }
-  int xo[S::P0];
-#pragma unroll
-  for (int i = 0; i < S::P0; ++i) xo[i] = int(wrap_add<T>(gx0, i, nfx));
 
-  P acc[S::NYR][S::P0];
+  P gre[S::NP], gim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1) of the row
   {
-    const i64 p = z0 + ((rb - z0) & (S::RZ - 1));
-    const C* plane = grid + (p % nfz) * nfy * nfx;
+    const i64 p = cta.z0 + ((rb - cta.z0) & (S::RZ - 1));
+    const C* row = grid + ((p % nfz) * nfy + row_y) * nfx;
 #pragma unroll
-    for (int j = 0; j < S::NYR; ++j) {
-#pragma unroll
-      for (int i = 0; i < S::P0; ++i) {
-        if (rowoff[j] >= 0) {
-          const C v = plane[rowoff[j] + xo[i]];
-          acc[j][i] = Ops::pack(v.x, v.y);
-        } else {
-          acc[j][i] = Ops::zero();
-        }
+    for (int q = 0; q < S::NP; ++q) {
+      C c0{T(0), T(0)}, c1{T(0), T(0)};
+      if (has_row) {
+        c0 = row[wrap_add(gx0, 2 * q, nfx)];
+        if (2 * q + 1 < S::P0) c1 = row[wrap_add(gx0, 2 * q + 1, nfx)];
       }
+      gre[q] = Ops::pack(c0.x, c1.x);
+      gim[q] = Ops::pack(c0.y, c1.y);
     }
   }
 
-  u32 e = bs[z0];
-  for (int t = z0; t < z1; ++t) {
+  u32 e = bs[cta.z0];
+  for (int t = cta.z0; t < cta.z1; ++t) {
     const u32 s = e;
     e = bs[t + 1];
     const int dz = (rb - t) & (S::RZ - 1);
-    const bool loader = dz == 0;  // holds plane t; reloads plane t + RZ afterwards
+    const bool loader = dz == 0 && has_row && t + 1 < cta.z1;  // reloads plane t + RZ
     __syncthreads();  // the previous plane's loaders have read the stage
-    if (loader && t + S::RZ < z1 + S::RZ - 1) {
-      const C* plane = grid + ((t + S::RZ) % nfz) * nfy * nfx;
+    if (loader) {
+      const C* row = grid + (((t + S::RZ) % nfz) * nfy + row_y) * nfx;
 #pragma unroll
-      for (int j = 0; j < S::NYR; ++j) {
-        if (rowoff[j] >= 0) {
-#pragma unroll
-          for (int i = 0; i < S::P0; ++i) cp_async_cell(&stage[ra][j][i], plane + rowoff[j] + xo[i]);
-        }
-      }
+      for (int i = 0; i < S::P0; ++i) cp_async_cell(&stage[ra][i], row + wrap_add(gx0, i, nfx));
       cp_async_commit();
     }
-    for (u32 base = s; base < e; base += S::NT) {
-      const int nb = int(min(e - base, u32(S::NT)));
-      u32 my_idx = 0;
+    for (u32 base = s; base < e; base += S::BATCH) {
+      const int nb = int(min(e - base, u32(S::BATCH)));
+      u32 my_perm = 0;
       if (tid < nb) {
-        const u32 p = base + tid;
-        my_idx = a.pts.perm[p];
-        stage_point<T, W, TX, false>(slots[tid], a.pts, p, C{T(0), T(0)}, a.beta, a.c);
+        const PointRec<T> rec = a.pts.rec[base + tid];
+        my_perm = rec.perm;
+        stage_point<T, W, TX, false>(slots[tid], rec, C{T(0), T(0)}, a.beta, a.c);
       }
       __syncthreads();
       for (int j0 = 0; j0 < nb; j0 += G) {
-        P part[G];
 #pragma unroll
         for (int k = 0; k < G; ++k) {
-          part[k] = Ops::zero();
-          if (j0 + k < nb && dz < W) {
-            const ZSlot<T, W, S::P0R>& sl = slots[j0 + k];
-            const P kz = Ops::splat(sl.kz[dz]);
+          C part{T(0), T(0)};
+          const int j = j0 + k;
+          if (j < nb) {
+            const Slot& sl = slots[j];
             const int ly = sl.ly;
-            P rs[S::NYR];
+            if (ly < a_lo + S::LA && ly + W > a_lo) {  // warp-uniform
+              const T wgt = sl.ky[ra] * sl.kz[dz];
+              P sr0 = Ops::zero(), sr1 = Ops::zero(), si0 = Ops::zero(), si1 = Ops::zero();
 #pragma unroll
-            for (int r = 0; r < S::NYR; ++r) rs[r] = Ops::zero();
-            if (sizeof(T) == 4) {
-#pragma unroll
-              for (int i = 0; i < S::P0; i += 2) {
-                const ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(&sl.kx[i]);
-                const P k0 = reinterpret_cast<const P&>(kk.x);
-                const P k1 = reinterpret_cast<const P&>(kk.y);
-#pragma unroll
-                for (int r = 0; r < S::NYR; ++r) {
-                  rs[r] = Ops::fma(k0, acc[r][i], rs[r]);
-                  if (i + 1 < S::P0) rs[r] = Ops::fma(k1, acc[r][i + 1], rs[r]);
+              for (int q = 0; q < S::NP; q += 2) {
+                P kk[2];
+                load_pairs<T>(&sl.kx[2 * q], kk);
+                sr0 = Ops::fma(kk[0], gre[q], sr0);
+                si0 = Ops::fma(kk[0], gim[q], si0);
+                if (q + 1 < S::NP) {
+                  sr1 = Ops::fma(kk[1], gre[q + 1], sr1);
+                  si1 = Ops::fma(kk[1], gim[q + 1], si1);
                 }
               }
-            } else {
-#pragma unroll
-              for (int i = 0; i < S::P0; ++i) {
-                const P k0 = sl.kx[i];
-#pragma unroll
-                for (int r = 0; r < S::NYR; ++r) rs[r] = Ops::fma(k0, acc[r][i], rs[r]);
-              }
-            }
-#pragma unroll
-            for (int r = 0; r < S::NYR; ++r) {
-              const int dy = ra + S::RY * r - ly;
-              const int dyc = dy < 0 ? 0 : (dy >= W ? W - 1 : dy);
-              const P kv = sl.kyv[dyc];
-              const P wgt = (dy >= 0 && dy < W) ? Ops::mul(kv, kz) : Ops::zero();
-              part[k] = Ops::fma(wgt, rs[r], part[k]);
+              const P sr = Ops::add(sr0, sr1);
+              const P si = Ops::add(si0, si1);
+              part = C{wgt * (Ops::lo(sr) + Ops::hi(sr)), wgt * (Ops::lo(si) + Ops::hi(si))};
             }
           }
+          red[warp][k][lane] = part;
         }
-        // Transposed butterfly: after it, lanes with (lane & 3) == 0 hold the warp sum of
-        // point j0 + ((lane >> 2) & 7).
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const bool hi = lane & 16;
-          const P send = hi ? part[k] : part[k + 4];
-          const P keep = hi ? part[k + 4] : part[k];
-          part[k] = Ops::add(keep, Ops::shfl_xor(send, 16));
-        }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const bool hi = lane & 8;
-          const P send = hi ? part[k] : part[k + 2];
-          const P keep = hi ? part[k + 2] : part[k];
-          part[k] = Ops::add(keep, Ops::shfl_xor(send, 8));
-        }
+        __syncwarp();
         {
-          const bool hi = lane & 4;
-          const P send = hi ? part[0] : part[1];
-          const P keep = hi ? part[1] : part[0];
-          part[0] = Ops::add(keep, Ops::shfl_xor(send, 4));
+          // lane (k, quarter): sum of 8 lanes' partials of point j0 + k, then over quarters
+          const int k = lane & (G - 1);
+          const int q4 = lane / G;
+          C sum{T(0), T(0)};
+#pragma unroll
+          for (int i = 0; i < 32 / 4; ++i) {
+            const C v = red[warp][k][q4 * 8 + i];
+            sum.x += v.x;
+            sum.y += v.y;
+          }
+#pragma unroll
+          for (int o = G; o < 32; o <<= 1) {
+            sum.x += __shfl_xor_sync(0xffffffffu, sum.x, o);
+            sum.y += __shfl_xor_sync(0xffffffffu, sum.y, o);
+          }
+          if (q4 == 0) res[warp][j0 + k] = sum;
         }
-        part[0] = Ops::add(part[0], Ops::shfl_xor(part[0], 2));
-        part[0] = Ops::add(part[0], Ops::shfl_xor(part[0], 1));
-        if ((lane & 3) == 0) res[warp][j0 + ((lane >> 2) & 7)] = part[0];
+        __syncwarp();
       }
       __syncthreads();
       if (tid < nb) {
-        P sum = res[0][tid];
+        C r = res[0][tid];
 #pragma unroll
-        for (int w = 1; w < NW; ++w) sum = Ops::add(sum, res[w][tid]);
-        C r = Ops::unpack(sum);
-        if (a.postphase) r = cmul(r, a.postphase[my_idx]);
-        a.out[my_idx] = r;
+        for (int w = 1; w < S::NWARP; ++w) {
+          r.x += res[w][tid].x;
+          r.y += res[w][tid].y;
+        }
+        if (a.postphase) r = cmul(r, a.postphase[my_perm]);
+        a.out[my_perm] = r;
       }
     }
-    if (loader && t + S::RZ < z1 + S::RZ - 1) {
+    if (loader) {
       cp_async_wait_all();
 #pragma unroll
-      for (int j = 0; j < S::NYR; ++j) {
-#pragma unroll
-        for (int i = 0; i < S::P0; ++i) {
-          if (rowoff[j] >= 0) {
-            const C v = stage[ra][j][i];
-            acc[j][i] = Ops::pack(v.x, v.y);
-          }
-        }
+      for (int q = 0; q < S::NP; ++q) {
+        const C c0 = stage[ra][2 * q];
+        const C c1 = stage[ra][2 * q + 1];
+        gre[q] = Ops::pack(c0.x, c1.x);
+        gim[q] = Ops::pack(c0.y, c1.y);
       }
     }
   }
