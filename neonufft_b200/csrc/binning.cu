@@ -90,7 +90,8 @@ __global__ void __launch_bounds__(kBinBlock)
     const u32 pos = bin_start[tile_lin] + ranks[i];
     PointRec<T> r;
     r.perm = u32(i);
-    r.local = pack_local(DIM, l[0], l[1], l[2]);
+    r.local = (DIM == 3 && g.zmajor) ? pack_local_zmajor(l[0], l[1], i0[2])
+                                     : pack_local(DIM, l[0], l[1], l[2]);
     r.frac[0] = T(fr[0]);
     r.frac[1] = T(fr[1]);
     r.frac[2] = T(fr[2]);

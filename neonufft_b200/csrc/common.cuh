@@ -121,6 +121,12 @@ __host__ __device__ __forceinline__ void unpack_local(int dim, u32 v, int& lx, i
 }
 constexpr int kMaxTileBits3[3] = {11, 11, 10};
 
+// Plane-major 3D point sets (BinGeom::zmajor; tiles of at most 16 x 16 x 1 cells) store the
+// absolute first kernel plane instead of the tile-local z: x 4 bits, y 4 bits, plane 24 bits.
+__host__ __device__ __forceinline__ u32 pack_local_zmajor(int lx, int ly, i64 plane) {
+  return u32(lx) | (u32(ly) << 4) | (u32(plane) << 8);
+}
+
 // One bin-sorted point: 32 bytes (a full 32-byte sector) for float and double plans, so that
 // the binning scatter writes each point with one sector and the kernels read it with two
 // 16-byte loads.

@@ -337,6 +337,9 @@ BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* 
     g.total_tiles *= g.ntiles[d];
   }
   if (g.total_tiles > i64(0x7fffffff)) throw_input("too many tiles");
+  if (g.zmajor && (g.tile[0] > 16 || g.tile[1] > 16 || g.tile[2] != 1 || g.nf[2] >= (i64(1) << 24))) {
+    throw_input("plane-major binning needs tiles of at most 16 x 16 x 1 and fewer than 2^24 planes");
+  }
   return g;
 }
 

@@ -6,27 +6,30 @@
 // point reading w^3 cells from global memory).
 //
 // Points are binned by (x tile of TX cells, y tile of 8 cells, single z plane), and the bins of
-// one (x, y) column are consecutive in plane order (BinGeom::zmajor). One CTA walks one column
-// over a chunk of planes. Its region is P0 x P1 cells in (x, y), P0 = TX + w - 1 and
-// P1 = 8 + w - 1 <= 15, times a window of RZ >= w consecutive planes:
+// one (x, y) column are consecutive in plane order (BinGeom::zmajor), so the points of a column
+// and range of planes are one contiguous run of records. One CTA walks one column over a chunk
+// of planes. Its region is P0 x P1 cells in (x, y), P0 = TX + w - 1 and P1 = 8 + w - 1 <= 15,
+// times a window of RZ >= w consecutive planes [t, t + RZ):
 //  * thread (a, b) keeps in registers the whole region row y = a (P0 cells, as pairs of
-//    neighbouring cells) of the one window plane p = b (mod RZ). The 16 rows a are split over
-//    the warps, LA = 32 / RZ rows per warp, so for a point whose footprint covers rows
+//    neighbouring cells) of the window plane p = b (mod RZ). The 16 rows are split over the
+//    warps, LA = 32 / RZ rows per warp, so for a point whose footprint covers rows
 //    [ly, ly + w) a warp either owns some of them or skips the point with a warp-uniform
 //    branch; no thread holds a cell that another thread updates, so there are no atomics and
 //    no shared-memory traffic per cell;
-//  * the points of plane t are staged in shared memory (one thread per point): kx over the
-//    region's x range, strength * ky over the 16 rows and kz over the RZ planes, each zero
-//    outside the footprint, so that every thread applies them with fixed register indices and
-//    no range tests;
+//  * the run of points is staged in shared memory 64 at a time (double-buffered, one barrier
+//    per batch, spread over all warps): kx over the region's x range, ky over the 16 rows and
+//    kz over the RZ planes, each zero outside the footprint, so that every thread applies
+//    them with fixed register indices and no range tests;
 //  * each owning thread updates its row with packed two-float FMAs (fma.rn.f32x2 on sm_100a),
 //    one for the real and one for the imaginary parts of two neighbouring cells;
-//  * spreading: when plane t is complete, the threads holding it add it to the fine grid
-//    (float2 / double2 atomics: neighbouring columns and chunks overlap by the halo) and start
-//    on plane t + RZ;
-//  * interpolation: the threads holding plane t reload their rows with plane t + RZ, fetched
-//    with cp.async while plane t's points are processed; per point the row sums are reduced
-//    for eight points at a time through a per-warp shared-memory transpose, then over warps.
+//  * when the next point starts on a later plane, the window advances: spreading adds each
+//    completed plane to the fine grid (float2 / double2 atomics: neighbouring columns and
+//    chunks overlap by the halo); interpolation reloads the threads that held it with the
+//    plane RZ further on, prefetched with cp.async one plane ahead;
+//  * interpolation reduces the row sums of eight points at a time through a per-warp
+//    shared-memory transpose, then over warps.
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace nnb {
@@ -106,65 +109,58 @@ __device__ __forceinline__ void atomic_add_cplx(double2* p, double2 v) {
 }
 
 // ---- geometry ----------------------------------------------------------------------------------
-template <int W, int TX>
+template <typename T, int W, int TX>
 struct ZShape {
-  static constexpr int RZ = W <= 4 ? 4 : 8;   // window planes = z residues (>= W)
-  static constexpr int LA = 32 / RZ;          // rows per warp
-  static constexpr int RY = 16;               // region rows (>= P1)
+  static constexpr int RZ = W <= 4 ? 4 : 8;         // window planes = z residues (>= W)
+  static constexpr int LA = 32 / RZ;                // rows per warp
+  static constexpr int RY = 16;                     // region rows (>= P1)
   static constexpr int NWARP = RY / LA;
-  static constexpr int NT = 32 * NWARP;       // threads per CTA
-  static constexpr int TY = 8;                // tile y
-  static constexpr int P0 = TX + W - 1;       // region x extent (cells)
-  static constexpr int NP = (P0 + 1) / 2;     // cell pairs per row
-  static constexpr int KXN = 4 * ((NP + 1) / 2);  // staged kx values (16-byte multiple)
-  static constexpr int P1 = TY + W - 1;       // region y extent
-  static constexpr int BATCH = 64;            // points staged at a time
-  static constexpr int G = 8;                 // points reduced together (interpolation)
+  static constexpr int NT = 32 * NWARP;             // threads per CTA
+  static constexpr int TY = 8;                      // tile y
+  static constexpr int P0 = TX + W - 1;             // region x extent (cells)
+  static constexpr int NP = (P0 + 1) / 2;           // cell pairs per row
+  static constexpr int KXN = 4 * ((NP + 1) / 2);    // staged kx values (16-byte multiple)
+  static constexpr int P1 = TY + W - 1;             // region y extent
+  static constexpr int BATCH = sizeof(T) == 4 ? 64 : 32;  // points staged at a time
+  static constexpr int G = 8;                       // points reduced together (interpolation)
   static_assert(W <= RZ && P1 <= RY, "window smaller than the kernel footprint");
+  static_assert(BATCH % NWARP == 0 && BATCH / NWARP <= 32, "staging threads");
 };
 
 // Per-point data staged in shared memory (one slot per point of a batch).
-template <typename T, int W, int TX, bool SPREAD>
+template <typename T, int W, int TX>
 struct alignas(16) ZSlot {
-  using S = ZShape<W, TX>;
-  using KY = typename std::conditional<SPREAD, cplx_t<T>, T>::type;
-  T kx[S::KXN];     // kx over the region's x range, zero outside the footprint
-  KY ky[S::RY];     // spreading: strength * ky per region row; interpolation: ky
-  T kz[S::RZ];      // kz per window offset, zero beyond w
-  int ly;           // first footprint row
+  using S = ZShape<T, W, TX>;
+  T kx[S::KXN];    // kx over the region's x range, zero outside the footprint
+  T ky[S::RY];     // ky over the region rows, zero outside the footprint
+  T kz[S::RZ];     // kz per window offset, zero beyond w
+  cplx_t<T> v;     // strength (spreading)
+  int lyp;         // first footprint row | first footprint plane << 4
+  u32 perm;        // original point index
 };
 
-// Stages bin-sorted point p into slot `sl`; v is its strength (spreading only).
-template <typename T, int W, int TX, bool SPREAD>
-__device__ __forceinline__ void stage_point(ZSlot<T, W, TX, SPREAD>& sl, const PointRec<T>& rec,
+// Stages bin-sorted record `rec` (plane-major packing) into slot `sl`.
+template <typename T, int W, int TX>
+__device__ __forceinline__ void stage_point(ZSlot<T, W, TX>& sl, const PointRec<T>& rec,
                                             cplx_t<T> v, T beta, T c) {
-  using S = ZShape<W, TX>;
-  const int lx = int(rec.local & 0x7FFu);
-  const int ly = int((rec.local >> 11) & 0x7FFu);
+  using S = ZShape<T, W, TX>;
+  const u32 loc = rec.local;
+  const int lx = int(loc & 0xFu);
+  const int ly = int((loc >> 4) & 0xFu);
+  float4* z = reinterpret_cast<float4*>(sl.kx);  // kx and ky are contiguous, 16-byte multiples
 #pragma unroll
-  for (int i = 0; i < S::KXN; ++i) sl.kx[i] = T(0);
-#pragma unroll
-  for (int i = 0; i < S::RY; ++i) {
-    if constexpr (SPREAD) {
-      sl.ky[i] = cplx_t<T>{T(0), T(0)};
-    } else {
-      sl.ky[i] = T(0);
-    }
-  }
+  for (int i = 0; i < int((S::KXN + S::RY) * sizeof(T) / 16); ++i) z[i] = make_float4(0, 0, 0, 0);
 #pragma unroll
   for (int k = 0; k < W; ++k) sl.kx[lx + k] = es_eval_fast<T>(rec.frac[0] + T(k), beta, c);
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
-    const T ky = es_eval_fast<T>(rec.frac[1] + T(k), beta, c);
-    if constexpr (SPREAD) {
-      sl.ky[ly + k] = cplx_t<T>{v.x * ky, v.y * ky};
-    } else {
-      sl.ky[ly + k] = ky;
-    }
-  }
+  for (int k = 0; k < W; ++k) sl.ky[ly + k] = es_eval_fast<T>(rec.frac[1] + T(k), beta, c);
 #pragma unroll
-  for (int k = 0; k < S::RZ; ++k) sl.kz[k] = k < W ? es_eval_fast<T>(rec.frac[2] + T(k), beta, c) : T(0);
-  sl.ly = ly;
+  for (int k = 0; k < S::RZ; ++k) {
+    sl.kz[k] = k < W ? es_eval_fast<T>(rec.frac[2] + T(k), beta, c) : T(0);
+  }
+  sl.v = v;
+  sl.lyp = ly | int((loc >> 8) << 4);
+  sl.perm = rec.perm;
 }
 
 // Chunk of planes handled by one CTA.
@@ -173,123 +169,182 @@ struct ZChunks {
   int count;  // chunks per column
 };
 
+// base + off wrapped to [0, n) for 0 <= base < n, 0 <= off.
 __device__ __forceinline__ i64 wrap_add(i64 base, int off, i64 n) {
   i64 i = base + off;
   while (i >= n) i -= n;
   return i;
 }
 
-// CTA coordinates: column (tx, ty) and plane range [z0, z1); false if the chunk has no points.
+// Column gx0 + i wrapped to the grid; `narrow` when the grid is narrower than the region.
+__device__ __forceinline__ i64 wrap_x(i64 gx0, int i, i64 nfx, bool narrow) {
+  i64 x = gx0 + i;
+  if (narrow) {
+    while (x >= nfx) x -= nfx;
+  } else if (x >= nfx) {
+    x -= nfx;
+  }
+  return x;
+}
+
+// CTA coordinates: column (tx, ty), plane range [z0, z1) and its run of points [pbeg, pend).
 struct ZCta {
   int tx, ty, z0, z1;
-  i64 col;
+  u32 pbeg, pend;
 };
 __device__ __forceinline__ bool zcta(const BinGeom& g, const u32* bin_start, ZChunks ch,
-                                     ZCta& c, const u32*& bs) {
+                                     ZCta& c) {
   const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
   const int chunk = int(blockIdx.x / ncols);
-  c.col = blockIdx.x - i64(chunk) * ncols;
-  c.tx = int(c.col % g.ntiles[0]);
-  c.ty = int(c.col / g.ntiles[0]);
+  const i64 col = blockIdx.x - i64(chunk) * ncols;
+  c.tx = int(col % g.ntiles[0]);
+  c.ty = int(col / g.ntiles[0]);
   const int nz = g.ntiles[2];  // == nf[2]: single-plane tiles
   c.z0 = chunk * ch.len;
   c.z1 = min(c.z0 + ch.len, nz);
-  bs = bin_start + c.col * nz;
-  return c.z0 < c.z1 && bs[c.z0] != bs[c.z1];
+  if (c.z0 >= c.z1) return false;
+  const u32* bs = bin_start + col * nz;
+  c.pbeg = bs[c.z0];
+  c.pend = bs[c.z1];
+  return c.pbeg != c.pend;
 }
+
+// Thread layout shared by both kernels.
+template <typename T, int W, int TX>
+struct ZThread {
+  using S = ZShape<T, W, TX>;
+  int tid, warp, lane, ra, rb, a_lo;
+  int stage_j;  // batch slot this thread stages (< BATCH), or -1
+  __device__ __forceinline__ ZThread() {
+    tid = threadIdx.x;
+    warp = tid >> 5;
+    lane = tid & 31;
+    ra = warp * S::LA + lane % S::LA;  // region row
+    rb = lane / S::LA;                  // z residue
+    a_lo = warp * S::LA;                // first row of this warp
+    stage_j = lane < S::BATCH / S::NWARP ? lane * S::NWARP + warp : -1;
+  }
+  // Whether this warp owns rows of a footprint starting at row ly.
+  __device__ __forceinline__ bool owns(int ly) const { return ly < a_lo + S::LA && ly + W > a_lo; }
+};
 
 // ---- spreading ---------------------------------------------------------------------------------
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<W, TX>::NT)
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, sizeof(T) == 4 ? 8 : 4)
     spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch) {
-  using S = ZShape<W, TX>;
+  using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  using Slot = ZSlot<T, W, TX, true>;
-  __shared__ Slot slots[S::BATCH];
+  using Slot = ZSlot<T, W, TX>;
+  __shared__ Slot slots[2][S::BATCH];
 
   const BinGeom& g = a.g;
   ZCta cta;
-  const u32* bs;
-  if (!zcta(g, a.pts.bin_start, ch, cta, bs)) return;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  const int ra = warp * S::LA + lane % S::LA;  // region row
-  const int rb = lane / S::LA;                  // z residue
-  const int a_lo = warp * S::LA;                // first row of this warp
-
+  if (!zcta(g, a.pts.bin_start, ch, cta)) return;
+  const ZThread<T, W, TX> th;
   const int batch = blockIdx.y;
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
+  const bool narrow = nfx < S::P0;
+  const bool has_row = th.ra < S::P1;
+  const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
   const i64 gx0 = i64(cta.tx) * TX;
-  const i64 row_y = ra < S::P1 ? wrap_add(i64(cta.ty) * S::TY, ra, nfy) : 0;
 
-  P are[S::NP], aim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1)
+  P are[S::NP], aim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1) of the row
 #pragma unroll
   for (int q = 0; q < S::NP; ++q) are[q] = aim[q] = Ops::zero();
+  bool dirty = false;
 
-  // Adds this thread's row of plane p (absolute, may exceed nfz) to the grid and clears it.
-  auto flush = [&](i64 p) {
-    if (ra < S::P1) {
-      C* row = grid + ((p % nfz) * nfy + row_y) * nfx;
+  // Adds this thread's row of plane p (absolute; may exceed nfz) to the grid and clears it.
+  auto flush = [&](int p) {
+    if (has_row && dirty) {
+      C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
 #pragma unroll
       for (int q = 0; q < S::NP; ++q) {
-        const C v0{Ops::lo(are[q]), Ops::lo(aim[q])};
-        const C v1{Ops::hi(are[q]), Ops::hi(aim[q])};
-        are[q] = aim[q] = Ops::zero();
-        if (v0.x != T(0) || v0.y != T(0)) atomic_add_cplx(&row[wrap_add(gx0, 2 * q, nfx)], v0);
-        if (2 * q + 1 < S::P0 && (v1.x != T(0) || v1.y != T(0))) {
-          atomic_add_cplx(&row[wrap_add(gx0, 2 * q + 1, nfx)], v1);
+        atomic_add_cplx(&row[wrap_x(gx0, 2 * q, nfx, narrow)], C{Ops::lo(are[q]), Ops::lo(aim[q])});
+        if (2 * q + 1 < S::P0) {
+          atomic_add_cplx(&row[wrap_x(gx0, 2 * q + 1, nfx, narrow)],
+                          C{Ops::hi(are[q]), Ops::hi(aim[q])});
         }
+        are[q] = aim[q] = Ops::zero();
       }
+    }
+    dirty = false;
+  };
+
+  const u32 npts = cta.pend - cta.pbeg;
+  const int nbatch = int((npts + S::BATCH - 1) / S::BATCH);
+  auto stage = [&](int k) {
+    const u32 off = u32(k) * S::BATCH;
+    const int nb = int(min(npts - off, u32(S::BATCH)));
+    if (th.stage_j >= 0 && th.stage_j < nb) {
+      const PointRec<T> rec = a.pts.rec[cta.pbeg + off + th.stage_j];
+      C v = in[rec.perm];
+      if (a.prephase) v = cmul(v, a.prephase[rec.perm]);
+      stage_point<T, W, TX>(slots[k & 1][th.stage_j], rec, v, a.beta, a.c);
     }
   };
 
-  u32 e = bs[cta.z0];
-  for (int t = cta.z0; t < cta.z1; ++t) {
-    const u32 s = e;
-    e = bs[t + 1];
-    const int dz = (rb - t) & (S::RZ - 1);  // this thread's plane within the window
-    for (u32 base = s; base < e; base += S::BATCH) {
-      const int nb = int(min(e - base, u32(S::BATCH)));
-      if (tid < nb) {
-        const PointRec<T> rec = a.pts.rec[base + tid];
-        C v = in[rec.perm];
-        if (a.prephase) v = cmul(v, a.prephase[rec.perm]);
-        stage_point<T, W, TX, true>(slots[tid], rec, v, a.beta, a.c);
-      }
-      __syncthreads();
-      for (int j = 0; j < nb; ++j) {
-        const Slot& sl = slots[j];
-        const int ly = sl.ly;
-        if (ly < a_lo + S::LA && ly + W > a_lo) {  // warp-uniform: this warp owns footprint rows
-          const C kyv = sl.ky[ra];
-          const T kzv = sl.kz[dz];
-          const P wre = Ops::splat(kyv.x * kzv);
-          const P wim = Ops::splat(kyv.y * kzv);
+  stage(0);
+  __syncthreads();
+  int cur = slots[0][0].lyp >> 4;  // window start: the first point's plane
+  int dz = (th.rb - cur) & (S::RZ - 1);
+  for (int k = 0; k < nbatch; ++k) {
+    const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
+    const Slot* sb = slots[k & 1];
+    auto apply = [&](const Slot& sl, int lyp) {
+      if (th.owns(lyp & 15)) {
+        dirty = true;
+        const T kw = sl.ky[th.ra] * sl.kz[dz];
+        const C v = sl.v;
+        const P wre = Ops::splat(v.x * kw);
+        const P wim = Ops::splat(v.y * kw);
 #pragma unroll
-          for (int q = 0; q < S::NP; q += 2) {
-            P k[2];
-            load_pairs<T>(&sl.kx[2 * q], k);
+        for (int q = 0; q < S::NP; q += 2) {
+          P kk[2];
+          load_pairs<T>(&sl.kx[2 * q], kk);
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              if (q + u < S::NP) {
-                are[q + u] = Ops::fma(k[u], wre, are[q + u]);
-                aim[q + u] = Ops::fma(k[u], wim, aim[q + u]);
-              }
+          for (int u = 0; u < 2; ++u) {
+            if (q + u < S::NP) {
+              are[q + u] = Ops::fma(kk[u], wre, are[q + u]);
+              aim[q + u] = Ops::fma(kk[u], wim, aim[q + u]);
             }
           }
         }
       }
-      __syncthreads();
+    };
+    for (int j0 = 0; j0 < nb; j0 += S::G) {
+      // Points are plane-sorted: if the group's last point is on the window's first plane, so
+      // are all of them and the window does not move inside the group.
+      if ((sb[min(j0 + S::G, nb) - 1].lyp >> 4) == cur) {
+#pragma unroll
+        for (int kk = 0; kk < S::G; ++kk) {
+          if (j0 + kk < nb) apply(sb[j0 + kk], sb[j0 + kk].lyp);
+        }
+      } else {
+#pragma unroll 1
+        for (int j = j0; j < min(j0 + S::G, nb); ++j) {
+          const Slot& sl = sb[j];
+          const int lyp = sl.lyp;
+          const int tp = lyp >> 4;
+          if (tp != cur) {  // advance the window: planes [cur, tp) are complete
+            const int n = min(tp - cur, S::RZ);
+            for (int i = 0; i < n; ++i) {
+              if (th.rb == ((cur + i) & (S::RZ - 1))) flush(cur + i);
+            }
+            cur = tp;
+            dz = (th.rb - cur) & (S::RZ - 1);
+          }
+          apply(sl, lyp);
+        }
+      }
     }
-    if (dz == 0) flush(t);
+    if (k + 1 < nbatch) stage(k + 1);
+    __syncthreads();
   }
-  // planes [z1, z1 + w - 1) still hold contributions of this chunk's last planes
-  flush(cta.z1 + ((rb - cta.z1) & (S::RZ - 1)));
+  flush(cur + ((th.rb - cur) & (S::RZ - 1)));  // the rest of the window
 }
 
 // ---- interpolation -----------------------------------------------------------------------------
@@ -305,151 +360,202 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<W, TX>::NT)
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
     interp_zwin_kernel(InterpArgs<T> a, ZChunks ch) {
-  using S = ZShape<W, TX>;
+  using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  using Slot = ZSlot<T, W, TX, false>;
+  using Slot = ZSlot<T, W, TX>;
   constexpr int G = S::G;
   constexpr int RS = 33;  // odd row stride of the transpose buffer: conflict-free reads
-  __shared__ Slot slots[S::BATCH];
+  __shared__ Slot slots[2][S::BATCH];
   __shared__ C red[S::NWARP][G][RS];
-  __shared__ C res[S::NWARP][S::BATCH];
-  __shared__ C stage[S::RY][2 * S::NP];
+  __shared__ C res[2][S::NWARP][S::BATCH];
+  __shared__ C stage_row[S::RY][2 * S::NP];  // next plane of the loading threads' rows
 
   const BinGeom& g = a.g;
   ZCta cta;
-  const u32* bs;
-  if (!zcta(g, a.pts.bin_start, ch, cta, bs)) return;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  const int ra = warp * S::LA + lane % S::LA;
-  const int rb = lane / S::LA;
-  const int a_lo = warp * S::LA;
-  const bool has_row = ra < S::P1;
-
+  if (!zcta(g, a.pts.bin_start, ch, cta)) return;
+  const ZThread<T, W, TX> th;
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
+  const bool narrow = nfx < S::P0;
+  const bool has_row = th.ra < S::P1;
+  const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
   const i64 gx0 = i64(cta.tx) * TX;
-  const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, ra, nfy) : 0;
-  if (tid < S::RY) {
-    for (int i = S::P0; i < 2 * S::NP; ++i) stage[tid][i] = C{T(0), T(0)};  // padding cell
+  if (th.tid < S::RY) {
+    for (int i = S::P0; i < 2 * S::NP; ++i) stage_row[th.tid][i] = C{T(0), T(0)};  // padding
   }
 
-  P gre[S::NP], gim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1) of the row
-  {
-    const i64 p = cta.z0 + ((rb - cta.z0) & (S::RZ - 1));
-    const C* row = grid + ((p % nfz) * nfy + row_y) * nfx;
+  // Row values of the window plane: real / imaginary parts of cell pairs (2q, 2q + 1); rows
+  // outside the region stay zero.
+  P gre[S::NP], gim[S::NP];
+#pragma unroll
+  for (int q = 0; q < S::NP; ++q) gre[q] = gim[q] = Ops::zero();
+  auto load_row = [&](int p) {
+    if (!has_row) return;
+    const C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
 #pragma unroll
     for (int q = 0; q < S::NP; ++q) {
-      C c0{T(0), T(0)}, c1{T(0), T(0)};
-      if (has_row) {
-        c0 = row[wrap_add(gx0, 2 * q, nfx)];
-        if (2 * q + 1 < S::P0) c1 = row[wrap_add(gx0, 2 * q + 1, nfx)];
-      }
+      const C c0 = row[wrap_x(gx0, 2 * q, nfx, narrow)];
+      C c1{T(0), T(0)};
+      if (2 * q + 1 < S::P0) c1 = row[wrap_x(gx0, 2 * q + 1, nfx, narrow)];
       gre[q] = Ops::pack(c0.x, c1.x);
       gim[q] = Ops::pack(c0.y, c1.y);
     }
-  }
-
-  u32 e = bs[cta.z0];
-  for (int t = cta.z0; t < cta.z1; ++t) {
-    const u32 s = e;
-    e = bs[t + 1];
-    const int dz = (rb - t) & (S::RZ - 1);
-    const bool loader = dz == 0 && has_row && t + 1 < cta.z1;  // reloads plane t + RZ
-    __syncthreads();  // the previous plane's loaders have read the stage
-    if (loader) {
-      const C* row = grid + (((t + S::RZ) % nfz) * nfy + row_y) * nfx;
+  };
+  bool pending = false;  // a cp.async of this thread's next plane is in flight
+  auto prefetch = [&](int p) {
+    if (!has_row) return;
+    const C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
 #pragma unroll
-      for (int i = 0; i < S::P0; ++i) cp_async_cell(&stage[ra][i], row + wrap_add(gx0, i, nfx));
-      cp_async_commit();
+    for (int i = 0; i < S::P0; ++i) {
+      cp_async_cell(&stage_row[th.ra][i], row + wrap_x(gx0, i, nfx, narrow));
     }
-    for (u32 base = s; base < e; base += S::BATCH) {
-      const int nb = int(min(e - base, u32(S::BATCH)));
-      u32 my_perm = 0;
-      if (tid < nb) {
-        const PointRec<T> rec = a.pts.rec[base + tid];
-        my_perm = rec.perm;
-        stage_point<T, W, TX, false>(slots[tid], rec, C{T(0), T(0)}, a.beta, a.c);
+    cp_async_commit();
+    pending = true;
+  };
+  auto take_prefetched = [&]() {
+    cp_async_wait_all();
+    pending = false;
+#pragma unroll
+    for (int q = 0; q < S::NP; ++q) {
+      const C c0 = stage_row[th.ra][2 * q];
+      const C c1 = stage_row[th.ra][2 * q + 1];
+      gre[q] = Ops::pack(c0.x, c1.x);
+      gim[q] = Ops::pack(c0.y, c1.y);
+    }
+  };
+
+  const u32 npts = cta.pend - cta.pbeg;
+  const int nbatch = int((npts + S::BATCH - 1) / S::BATCH);
+  auto stage = [&](int k) {
+    const u32 off = u32(k) * S::BATCH;
+    const int nb = int(min(npts - off, u32(S::BATCH)));
+    if (th.stage_j >= 0 && th.stage_j < nb) {
+      stage_point<T, W, TX>(slots[k & 1][th.stage_j], a.pts.rec[cta.pbeg + off + th.stage_j],
+                            C{T(0), T(0)}, a.beta, a.c);
+    }
+  };
+  // Writes the outputs of batch k: this thread's staged point, whose slot only this thread's
+  // next staging rewrites.
+  auto output = [&](int k) {
+    const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
+    const int j = th.stage_j;
+    if (j >= 0 && j < nb) {
+      C r = res[k & 1][0][j];
+#pragma unroll
+      for (int w = 1; w < S::NWARP; ++w) {
+        r.x += res[k & 1][w][j].x;
+        r.y += res[k & 1][w][j].y;
       }
-      __syncthreads();
-      for (int j0 = 0; j0 < nb; j0 += G) {
+      const u32 perm = slots[k & 1][j].perm;
+      if (a.postphase) r = cmul(r, a.postphase[perm]);
+      a.out[perm] = r;
+    }
+  };
+
+  stage(0);
+  __syncthreads();
+  int cur = slots[0][0].lyp >> 4;  // window start: the first point's plane
+  int dz = (th.rb - cur) & (S::RZ - 1);
+  load_row(cur + dz);
+  if (dz == 0) prefetch(cur + S::RZ);
+
+  for (int k = 0; k < nbatch; ++k) {
+    const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
+    const Slot* sb = slots[k & 1];
+    auto partial = [&](const Slot& sl, int lyp) -> C {
+      if (!th.owns(lyp & 15)) return C{T(0), T(0)};
+      const T kw = sl.ky[th.ra] * sl.kz[dz];
+      P sr0 = Ops::zero(), sr1 = Ops::zero(), si0 = Ops::zero(), si1 = Ops::zero();
 #pragma unroll
-        for (int k = 0; k < G; ++k) {
+      for (int q = 0; q < S::NP; q += 2) {
+        P kp[2];
+        load_pairs<T>(&sl.kx[2 * q], kp);
+        sr0 = Ops::fma(kp[0], gre[q], sr0);
+        si0 = Ops::fma(kp[0], gim[q], si0);
+        if (q + 1 < S::NP) {
+          sr1 = Ops::fma(kp[1], gre[q + 1], sr1);
+          si1 = Ops::fma(kp[1], gim[q + 1], si1);
+        }
+      }
+      const P sr = Ops::add(sr0, sr1);
+      const P si = Ops::add(si0, si1);
+      return C{kw * (Ops::lo(sr) + Ops::hi(sr)), kw * (Ops::lo(si) + Ops::hi(si))};
+    };
+    for (int j0 = 0; j0 < nb; j0 += G) {
+      // Points are plane-sorted: if the group's last point is on the window's first plane, so
+      // are all of them and the window does not move inside the group.
+      if ((sb[min(j0 + G, nb) - 1].lyp >> 4) == cur) {
+#pragma unroll
+        for (int kk = 0; kk < G; ++kk) {
+          const int j = j0 + kk;
+          red[th.warp][kk][th.lane] = j < nb ? partial(sb[j], sb[j].lyp) : C{T(0), T(0)};
+        }
+      } else {
+#pragma unroll 1
+        for (int kk = 0; kk < G; ++kk) {
           C part{T(0), T(0)};
-          const int j = j0 + k;
+          const int j = j0 + kk;
           if (j < nb) {
-            const Slot& sl = slots[j];
-            const int ly = sl.ly;
-            if (ly < a_lo + S::LA && ly + W > a_lo) {  // warp-uniform
-              const T wgt = sl.ky[ra] * sl.kz[dz];
-              P sr0 = Ops::zero(), sr1 = Ops::zero(), si0 = Ops::zero(), si1 = Ops::zero();
-#pragma unroll
-              for (int q = 0; q < S::NP; q += 2) {
-                P kk[2];
-                load_pairs<T>(&sl.kx[2 * q], kk);
-                sr0 = Ops::fma(kk[0], gre[q], sr0);
-                si0 = Ops::fma(kk[0], gim[q], si0);
-                if (q + 1 < S::NP) {
-                  sr1 = Ops::fma(kk[1], gre[q + 1], sr1);
-                  si1 = Ops::fma(kk[1], gim[q + 1], si1);
+            const Slot& sl = sb[j];
+            const int lyp = sl.lyp;
+            const int tp = lyp >> 4;
+            if (tp != cur) {  // advance the window: rows of planes [cur, tp) move on by RZ
+              if (tp - cur >= S::RZ) {
+                if (pending) cp_async_wait_all();
+                pending = false;
+                load_row(tp + ((th.rb - tp) & (S::RZ - 1)));
+              } else {
+                for (int i = 0; i < tp - cur; ++i) {
+                  if (th.rb == ((cur + i) & (S::RZ - 1))) {
+                    if (pending) {
+                      take_prefetched();
+                    } else {
+                      load_row(cur + i + S::RZ);
+                    }
+                  }
                 }
               }
-              const P sr = Ops::add(sr0, sr1);
-              const P si = Ops::add(si0, si1);
-              part = C{wgt * (Ops::lo(sr) + Ops::hi(sr)), wgt * (Ops::lo(si) + Ops::hi(si))};
+              __syncwarp();  // the staged rows are read before the next prefetch rewrites them
+              cur = tp;
+              dz = (th.rb - cur) & (S::RZ - 1);
+              if (dz == 0) prefetch(cur + S::RZ);
             }
+            part = partial(sl, lyp);
           }
-          red[warp][k][lane] = part;
+          red[th.warp][kk][th.lane] = part;
         }
-        __syncwarp();
-        {
-          // lane (k, quarter): sum of 8 lanes' partials of point j0 + k, then over quarters
-          const int k = lane & (G - 1);
-          const int q4 = lane / G;
-          C sum{T(0), T(0)};
-#pragma unroll
-          for (int i = 0; i < 32 / 4; ++i) {
-            const C v = red[warp][k][q4 * 8 + i];
-            sum.x += v.x;
-            sum.y += v.y;
-          }
-#pragma unroll
-          for (int o = G; o < 32; o <<= 1) {
-            sum.x += __shfl_xor_sync(0xffffffffu, sum.x, o);
-            sum.y += __shfl_xor_sync(0xffffffffu, sum.y, o);
-          }
-          if (q4 == 0) res[warp][j0 + k] = sum;
-        }
-        __syncwarp();
       }
-      __syncthreads();
-      if (tid < nb) {
-        C r = res[0][tid];
+      __syncwarp();
+      {
+        // lane (k8, quarter): sum of 8 lanes' partials of point j0 + k8, then over quarters
+        const int k8 = th.lane & (G - 1);
+        const int q4 = th.lane / G;
+        C sum{T(0), T(0)};
 #pragma unroll
-        for (int w = 1; w < S::NWARP; ++w) {
-          r.x += res[w][tid].x;
-          r.y += res[w][tid].y;
+        for (int i = 0; i < 8; ++i) {
+          const C v = red[th.warp][k8][q4 * 8 + i];
+          sum.x += v.x;
+          sum.y += v.y;
         }
-        if (a.postphase) r = cmul(r, a.postphase[my_perm]);
-        a.out[my_perm] = r;
+#pragma unroll
+        for (int o = G; o < 32; o <<= 1) {
+          sum.x += __shfl_xor_sync(0xffffffffu, sum.x, o);
+          sum.y += __shfl_xor_sync(0xffffffffu, sum.y, o);
+        }
+        if (q4 == 0) res[k & 1][th.warp][j0 + k8] = sum;
       }
+      __syncwarp();
     }
-    if (loader) {
-      cp_async_wait_all();
-#pragma unroll
-      for (int q = 0; q < S::NP; ++q) {
-        const C c0 = stage[ra][2 * q];
-        const C c1 = stage[ra][2 * q + 1];
-        gre[q] = Ops::pack(c0.x, c1.x);
-        gim[q] = Ops::pack(c0.y, c1.y);
-      }
-    }
+    if (k > 0) output(k - 1);
+    if (k + 1 < nbatch) stage(k + 1);
+    __syncthreads();
   }
+  output(nbatch - 1);
+  if (pending) cp_async_wait_all();
 }
 
 ZChunks make_chunks(i64 ncols, int nz, int w) {
@@ -469,7 +575,7 @@ ZChunks make_chunks(i64 ncols, int nz, int w) {
 
 template <typename T, int W, int TX>
 void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
-  using S = ZShape<W, TX>;
+  using S = ZShape<T, W, TX>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const i64 ctas = ncols * ch.count;
@@ -481,7 +587,7 @@ void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
 
 template <typename T, int W, int TX>
 void launch_interp_zwin_tw(const InterpArgs<T>& a, cudaStream_t stream) {
-  using S = ZShape<W, TX>;
+  using S = ZShape<T, W, TX>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const i64 ctas = ncols * ch.count;
