@@ -181,6 +181,8 @@ def main():
     ap.add_argument("--samples", type=int, default=10000)
     ap.add_argument("--spread-method", type=int, default=0,
                     help="engine spreading/interpolation method (0 = plan default)")
+    ap.add_argument("--tile", default="",
+                    help="engine tile shape, e.g. 4,8,1 (default: the plan's choice)")
     ap.add_argument("--n-spread", type=int, default=-1,
                     help="kernel width (0 = reference heuristic; default: the tuned width)")
     args = ap.parse_args()
@@ -222,7 +224,8 @@ def main():
     # The reference heuristic gives w = 7 at tol 1e-6, whose truncation error alone is ~1.5e-6
     # rel-l2 (even in FP64); the tuned width w = 8 meets rel-l2 <= 1e-6, the metric's bar.
     n_spread = wl.get("tuned_w", 0) if args.n_spread < 0 else args.n_spread
-    opt = nnb.Options(tol=tol, spread_method=args.spread_method, n_spread=n_spread)
+    tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 0, 0)
+    opt = nnb.Options(tol=tol, spread_method=args.spread_method, n_spread=n_spread, tile=tile)
     plan = nnb.Plan(opt, -1, M, loc, modes)
     info = plan.info()
 

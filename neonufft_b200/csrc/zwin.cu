@@ -230,7 +230,7 @@ struct ZThread {
 
 // ---- spreading ---------------------------------------------------------------------------------
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, sizeof(T) == 4 ? 8 : 4)
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
     spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch) {
   using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
@@ -315,31 +315,19 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT, sizeof(T) == 4 ? 8 : 4)
         }
       }
     };
-    for (int j0 = 0; j0 < nb; j0 += S::G) {
-      // Points are plane-sorted: if the group's last point is on the window's first plane, so
-      // are all of them and the window does not move inside the group.
-      if ((sb[min(j0 + S::G, nb) - 1].lyp >> 4) == cur) {
-#pragma unroll
-        for (int kk = 0; kk < S::G; ++kk) {
-          if (j0 + kk < nb) apply(sb[j0 + kk], sb[j0 + kk].lyp);
+    for (int j = 0; j < nb; ++j) {
+      const Slot& sl = sb[j];
+      const int lyp = sl.lyp;
+      const int tp = lyp >> 4;
+      if (tp != cur) {  // advance the window: planes [cur, tp) are complete
+        const int n = min(tp - cur, S::RZ);
+        for (int i = 0; i < n; ++i) {
+          if (th.rb == ((cur + i) & (S::RZ - 1))) flush(cur + i);
         }
-      } else {
-#pragma unroll 1
-        for (int j = j0; j < min(j0 + S::G, nb); ++j) {
-          const Slot& sl = sb[j];
-          const int lyp = sl.lyp;
-          const int tp = lyp >> 4;
-          if (tp != cur) {  // advance the window: planes [cur, tp) are complete
-            const int n = min(tp - cur, S::RZ);
-            for (int i = 0; i < n; ++i) {
-              if (th.rb == ((cur + i) & (S::RZ - 1))) flush(cur + i);
-            }
-            cur = tp;
-            dz = (th.rb - cur) & (S::RZ - 1);
-          }
-          apply(sl, lyp);
-        }
+        cur = tp;
+        dz = (th.rb - cur) & (S::RZ - 1);
       }
+      apply(sl, lyp);
     }
     if (k + 1 < nbatch) stage(k + 1);
     __syncthreads();
