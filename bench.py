@@ -46,6 +46,11 @@ WORKLOADS = {
                dim=2, M=100_000, N=256, tol=1e-6, types=(1,), seed=1, cpu_sample=100_000,
                tuned_w=8),
 }
+# DRAM bytes (read + write) per point of one launch of the dominant kernel, from one ncu capture
+# of the same configuration (profiles/zwin_c2.md): (workload, precision, method, n_spread, tile,
+# kernel) -> bytes per point.
+DRAM_BYTES_PER_POINT = {}
+
 METRIC = "NU points/sec per transform at rel-l2 <=1e-6 (tuned FP32 vs plain GPU; CPU ref)"
 UNIT = "points/s"
 
@@ -59,57 +64,94 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event reasons of the benchmark's GPU, sampled every 10 ms through NVML
+    during the timed region (nvidia-smi as the fallback when NVML is unavailable)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40), ("sw_power_cap", 0x4))
 
     def __init__(self, device_index: int):
         self.idx = device_index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self.source = "nvml"
+        self._stop = threading.Event()
+        self._t = None
+        self._proc = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.idx)
+        try:
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+
+    def _run(self, h):
+        import pynvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, bit in self.REASONS:
+                    if bits & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.01)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            import pynvml
+            h = self._handle()
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self._t = threading.Thread(target=self._run, args=(h,), daemon=True)
+            self._t.start()
         except Exception:
-            self.proc = None
+            self.source = "nvidia-smi"
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.idx),
+                     "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                     "clocks_event_reasons.sw_thermal_slowdown,"
+                     "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                     "--format=csv,noheader,nounits", "-lms", "100"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._t = threading.Thread(target=self._read_smi, daemon=True)
+                self._t.start()
+            except Exception:
+                self._proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _read_smi(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            try:
+                self.samples.append(float(parts[0]))
+                self.max_mhz = float(parts[1])
+            except (ValueError, IndexError):
+                continue
+            for (name, _), v in zip(self.REASONS, parts[2:6]):
+                if v.lower().startswith("active"):
+                    self.reasons.add(name)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
-                continue
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                sm.append(float(parts[0]))
-                smax = float(parts[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        sm.sort()
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=5)
+        sm = sorted(self.samples)
         med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(sm), "source": self.source}
 
 
 def dist_setup():
@@ -172,7 +214,7 @@ def run_reference(args, wl):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
@@ -181,6 +223,8 @@ def main():
     ap.add_argument("--samples", type=int, default=10000)
     ap.add_argument("--spread-method", type=int, default=0,
                     help="engine spreading/interpolation method (0 = plan default)")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                    help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
     ap.add_argument("--tile", default="",
                     help="engine tile shape, e.g. 4,8,1 (default: the plan's choice)")
     ap.add_argument("--n-spread", type=int, default=-1,
@@ -210,15 +254,19 @@ def main():
     dim, M, N, tol = wl["dim"], wl["M"], wl["N"], wl["tol"]
     g = torch.Generator(device="cuda")
     g.manual_seed(wl["seed"] + 97 * rank)
-    loc = [(torch.rand(M, generator=g, device="cuda", dtype=torch.float32) * 2 - 1) * math.pi
+    f64 = args.precision == "f64"
+    rdt = torch.float64 if f64 else torch.float32
+    cdt = torch.complex128 if f64 else torch.complex64
+    rsz = 8 if f64 else 4  # bytes per real
+    loc = [(torch.rand(M, generator=g, device="cuda", dtype=rdt) * 2 - 1) * math.pi
            for _ in range(dim)]
-    c = torch.complex(torch.randn(M, generator=g, device="cuda"),
-                      torch.randn(M, generator=g, device="cuda"))
+    c = torch.complex(torch.randn(M, generator=g, device="cuda", dtype=rdt),
+                      torch.randn(M, generator=g, device="cuda", dtype=rdt))
     nm = N ** dim
-    f = torch.complex(torch.randn(nm, generator=g, device="cuda"),
-                      torch.randn(nm, generator=g, device="cuda"))
-    out1 = torch.empty(nm, dtype=torch.complex64, device="cuda")
-    out2 = torch.empty(M, dtype=torch.complex64, device="cuda")
+    f = torch.complex(torch.randn(nm, generator=g, device="cuda", dtype=rdt),
+                      torch.randn(nm, generator=g, device="cuda", dtype=rdt))
+    out1 = torch.empty(nm, dtype=cdt, device="cuda")
+    out2 = torch.empty(M, dtype=cdt, device="cuda")
     strides = [1, N, N * N][:dim]
     modes = [N] * dim
     # The reference heuristic gives w = 7 at tol 1e-6, whose truncation error alone is ~1.5e-6
@@ -272,19 +320,21 @@ def main():
 
     # ---- end-to-end through the public API with host buffers --------------------------------
     pin = dict(device="cpu", pin_memory=True)
-    loc_h = [torch.empty(M, dtype=torch.float32, **pin) for _ in range(dim)]
+    loc_h = [torch.empty(M, dtype=rdt, **pin) for _ in range(dim)]
     for a, b in zip(loc_h, loc):
         a.copy_(b)
-    c_h = torch.empty(M, dtype=torch.complex64, **pin)
+    c_h = torch.empty(M, dtype=cdt, **pin)
     c_h.copy_(c)
-    f_h = torch.empty(nm, dtype=torch.complex64, **pin)
+    f_h = torch.empty(nm, dtype=cdt, **pin)
     f_h.copy_(f)
-    o1_h = torch.empty(nm, dtype=torch.complex64, **pin)
-    o2_h = torch.empty(M, dtype=torch.complex64, **pin)
+    o1_h = torch.empty(nm, dtype=cdt, **pin)
+    o2_h = torch.empty(M, dtype=cdt, **pin)
     loc_d = [torch.empty_like(a) for a in loc]
     c_d, f_d = torch.empty_like(c), torch.empty_like(f)
-    h2d = dim * M * 4 + (M * 8 if 1 in wl["types"] else 0) + (nm * 8 if 2 in wl["types"] else 0)
-    d2h = (nm * 8 if 1 in wl["types"] else 0) + (M * 8 if 2 in wl["types"] else 0)
+    csz = 2 * rsz
+    h2d = (dim * M * rsz + (M * csz if 1 in wl["types"] else 0)
+           + (nm * csz if 2 in wl["types"] else 0))
+    d2h = (nm * csz if 1 in wl["types"] else 0) + (M * csz if 2 in wl["types"] else 0)
 
     def e2e_step():
         for a, b in zip(loc_d, loc_h):
@@ -350,22 +400,25 @@ def main():
     interp_ms = stages["interp"][0] / max(1, stages["interp"][1]) if stages["interp"][1] else 0.0
     w = info["n_spread"]
     nf_cells = int(np.prod(info["grid"][:dim]))
-    # algorithmic bytes of one spread launch: per point perm + packed cell + dim fractions
-    # (4 B each) + its complex64 strength, plus one write of the complex64 fine grid.
-    spread_bytes = M * (4 + 4 + 4 * dim + 8) + nf_cells * 8
+    # Algorithmic bytes of one launch: per point its 32-byte bin-sorted record and its complex
+    # strength (spreading) or output (interpolation), plus one pass over the complex fine grid.
+    csz = 16 if f64 else 8
+    spread_bytes = M * (32 + csz) + nf_cells * csz
     spread_flop = M * 5 * w ** dim
     dom = "spread"
     dom_ms, dom_bytes, dom_flop = spread_ms, spread_bytes, spread_flop
     if interp_ms > spread_ms:
         dom = "interp"
         dom_ms = interp_ms
-        dom_bytes = M * (4 + 4 + 4 * dim + 8) + nf_cells * 8
+        dom_bytes = M * (32 + csz) + nf_cells * csz
         dom_flop = M * 5 * w ** dim
+    key = (args.workload, args.precision, info["spread_method"], w, tuple(info["tile"][:dim]), dom)
+    traffic = (DRAM_BYTES_PER_POINT[key] * M) if key in DRAM_BYTES_PER_POINT else None
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
     roofline = {
         "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} HBM copy",
+        "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} HBM copy",
         "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
         "fp32": {"achieved_tflops": dom_flop / (dom_ms * 1e-3) / 1e12,
                  "peak_tflops_nominal": fp32_peak,
@@ -392,11 +445,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic (seeded uniform points, N(0,1) strengths and modes)",
             "config": {"workload": wl["name"], "M": M, "N": N, "dim": dim, "tol": tol,
                        "upsampfac": 2.0, "n_spread": w, "fine_grid": info["grid"][:dim],
                        "tile": info["tile"][:dim], "method": info["spread_method"],
+                       "precision": args.precision,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (126 MB); no flush"},
             "clocks": clk,

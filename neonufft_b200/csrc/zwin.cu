@@ -129,7 +129,7 @@ struct ZShape {
 
 // Per-point data staged in shared memory (one slot per point of a batch).
 template <typename T, int W, int TX>
-struct alignas(16) ZSlot {
+struct alignas(16) ZSlotFields {
   using S = ZShape<T, W, TX>;
   T kx[S::KXN];    // kx over the region's x range, zero outside the footprint
   T ky[S::RY];     // ky over the region rows, zero outside the footprint
@@ -138,6 +138,17 @@ struct alignas(16) ZSlot {
   int lyp;         // first footprint row | first footprint plane << 4
   u32 perm;        // original point index
 };
+// 16 bytes of padding when the fields span an even number of 16-byte units: with an odd slot
+// stride, consecutive lanes staging consecutive slots store to different banks.
+template <bool ODD>
+struct ZSlotPad {
+  int pad[4];
+};
+template <>
+struct ZSlotPad<true> {};
+template <typename T, int W, int TX>
+struct alignas(16) ZSlot
+    : ZSlotFields<T, W, TX>, ZSlotPad<(sizeof(ZSlotFields<T, W, TX>) / 16) % 2 == 1> {};
 
 // Stages bin-sorted record `rec` (plane-major packing) into slot `sl`.
 template <typename T, int W, int TX>
@@ -222,7 +233,9 @@ struct ZThread {
     ra = warp * S::LA + lane % S::LA;  // region row
     rb = lane / S::LA;                  // z residue
     a_lo = warp * S::LA;                // first row of this warp
-    stage_j = lane < S::BATCH / S::NWARP ? lane * S::NWARP + warp : -1;
+    // consecutive lanes stage consecutive slots (the slot stride is 4 words times an odd
+    // number, so their shared-memory stores fall in different banks)
+    stage_j = lane < S::BATCH / S::NWARP ? warp * (S::BATCH / S::NWARP) + lane : -1;
   }
   // Whether this warp owns rows of a footprint starting at row ly.
   __device__ __forceinline__ bool owns(int ly) const { return ly < a_lo + S::LA && ly + W > a_lo; }
