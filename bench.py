@@ -49,7 +49,10 @@ WORKLOADS = {
 # DRAM bytes (read + write) per point of one launch of the dominant kernel, from one ncu capture
 # of the same configuration (profiles/zwin_c2.md): (workload, precision, method, n_spread, tile,
 # kernel) -> bytes per point.
-DRAM_BYTES_PER_POINT = {}
+DRAM_BYTES_PER_POINT = {
+    ("c2", "f32", 3, 8, (8, 8, 1), "interp"): (659.360512e6 + 258.979328e6) / 1e7,
+    ("c2", "f32", 3, 8, (8, 8, 1), "spread"): (944.736256e6 + 132.786176e6) / 1e7,
+}
 
 METRIC = "NU points/sec per transform at rel-l2 <=1e-6 (tuned FP32 vs plain GPU; CPU ref)"
 UNIT = "points/s"
