@@ -42,6 +42,9 @@ WORKLOADS = {
     "ns": dict(name="3D type-1, M=1e8 uniform [-pi,pi)^3, N=256^3, tol 1e-6",
                dim=3, M=100_000_000, N=256, tol=1e-6, types=(1,), seed=7, cpu_sample=1_000_000,
                tuned_w=8),
+    "c4": dict(name="64 uneven 2D/3D type-1 transforms in one batch, M log-uniform [1e4,1e7], "
+                    "N per dim in {64,128,256,512} (3D <= 256), half Gaussian blobs (sigma 0.1), tol 1e-6",
+               batch=64, tol=1e-6, types=(1,), seed=4, tuned_w=8),
     "c1": dict(name="2D type-1, M=1e5 uniform [-pi,pi)^2, N=256^2, tol 1e-6",
                dim=2, M=100_000, N=256, tol=1e-6, types=(1,), seed=1, cpu_sample=100_000,
                tuned_w=8),
@@ -214,6 +217,155 @@ def run_reference(args, wl):
     return 0
 
 
+def batch_problems(wl, rank):
+    """The seeded problems of the batched workload (host arrays)."""
+    import numpy as np
+    rng = np.random.default_rng(wl["seed"] + 97 * rank)
+    probs = []
+    for i in range(wl["batch"]):
+        dim = 2 if i % 2 == 0 else 3
+        M = int(round(10 ** rng.uniform(4, 7)))
+        choices = [64, 128, 256, 512] if dim == 2 else [64, 128, 256]
+        modes = [int(rng.choice(choices))] * dim
+        if i % 4 >= 2:  # Gaussian blob wrapped into [-pi, pi)
+            centre = rng.uniform(-np.pi, np.pi, dim)
+            pts = [(np.mod(centre[d] + 0.1 * rng.standard_normal(M) + np.pi, 2 * np.pi) - np.pi)
+                   .astype(np.float32) for d in range(dim)]
+        else:
+            pts = [rng.uniform(-np.pi, np.pi, M).astype(np.float32) for _ in range(dim)]
+        c = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+        probs.append(dict(dim=dim, M=M, modes=modes, pts=pts, c=c))
+    return probs
+
+
+def run_batch(args, wl):
+    """Batched workload: one Batch of all transforms, timed in graph, streams and serial modes."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import neonufft_b200 as nnb
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    probs = batch_problems(wl, rank)
+    n_spread = wl.get("tuned_w", 0) if args.n_spread < 0 else args.n_spread
+    opt = nnb.Options(tol=wl["tol"], n_spread=n_spread)
+    batch = nnb.Batch(opt, torch.float32, num_streams=args.streams)
+    dev = []
+    for p in probs:
+        loc = [torch.from_numpy(x).cuda() for x in p["pts"]]
+        c = torch.from_numpy(p["c"]).cuda()
+        out = torch.empty(int(np.prod(p["modes"])), dtype=torch.complex64, device="cuda")
+        strides = [1, p["modes"][0], p["modes"][0] ** 2][:p["dim"]]
+        batch.add(1, -1, loc, p["modes"], c, out, strides)
+        dev.append((loc, c, out))
+    total = sum(p["M"] for p in probs)
+
+    def timed(mode):
+        for _ in range(args.warmup):
+            batch.execute(mode)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            batch.execute(mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    ms_serial = timed(nnb.Batch.SERIAL)
+    l0 = nnb.kernel_launches()
+    ms_streams = timed(nnb.Batch.STREAMS)
+    per_step = (nnb.kernel_launches() - l0) // max(1, args.steps + args.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_graph = timed(nnb.Batch.GRAPH)
+    clk = clocks.stop()
+    # the graph replays the kernels of one streams-mode execution per step
+    launches = per_step * args.steps
+
+    # end to end: strengths from pinned host memory, outputs back to pinned host memory
+    pin = dict(device="cpu", pin_memory=True)
+    c_h = [torch.from_numpy(p["c"]).pin_memory() for p in probs]
+    o_h = [torch.empty(d[2].numel(), dtype=torch.complex64, **pin) for d in dev]
+    h2d = sum(int(x.numel()) * 8 for x in c_h)
+    d2h = sum(int(x.numel()) * 8 for x in o_h)
+
+    def e2e():
+        for (loc, c, out), ch in zip(dev, c_h):
+            c.copy_(ch, non_blocking=True)
+        batch.execute(nnb.Batch.GRAPH)
+        for (loc, c, out), oh in zip(dev, o_h):
+            oh.copy_(out, non_blocking=True)
+
+    e2e()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        e2e()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+
+    acc = {}
+    if not args.no_accuracy:
+        worst = 0.0
+        gs = torch.Generator(device="cuda")
+        gs.manual_seed(123)
+        for i in range(0, len(probs), 8):  # every eighth transform, 2000 sampled modes
+            p = probs[i]
+            loc, c, out = dev[i]
+            N, dim = p["modes"][0], p["dim"]
+            idx = torch.randint(0, out.numel(), (2000,), generator=gs, device="cuda")
+            kk, rem = [], idx.clone()
+            for d in range(dim):
+                kk.append(rem % N - N // 2)
+                rem = rem // N
+            kidx = torch.stack(kk, dim=1).contiguous()
+            ref = torch.empty(2000, dtype=torch.complex128, device="cuda")
+            nnb.direct_type1_f64(-1, [a.double() for a in loc], c.to(torch.complex128), kidx, ref)
+            got = out[idx].to(torch.complex128)
+            worst = max(worst, float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref)))
+        acc = {"type1_rel_l2_max": worst, "transforms_checked": len(range(0, len(probs), 8)),
+               "samples_each": 2000}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * total / (ms_graph * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform and Gaussian-blob points, N(0,1) strengths)",
+            "config": {"workload": wl["name"], "transforms": len(probs), "points": total,
+                       "n_spread": n_spread, "streams": args.streams, "mode": "graph",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (126 MB); no flush"},
+            "modes_ms_per_step": {"serial": ms_serial, "streams": ms_streams, "graph": ms_graph},
+            "clocks": clk,
+            "e2e": {"value": world * total / (ms_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+            "gpu_launches": int(launches), "roofline": None, "cpu_baseline": None,
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,6 +380,7 @@ def main():
                     help="engine spreading/interpolation method (0 = plan default)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
+    ap.add_argument("--streams", type=int, default=8, help="internal streams of a batch (c4)")
     ap.add_argument("--tile", default="",
                     help="engine tile shape, e.g. 4,8,1 (default: the plan's choice)")
     ap.add_argument("--n-spread", type=int, default=-1,
@@ -236,7 +389,13 @@ def main():
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if "batch" in wl:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the batched workload has no CPU reference arm"}))
+            return 0
         return run_reference(args, wl)
+    if "batch" in wl:
+        return run_batch(args, wl)
 
     import numpy as np
     import torch

@@ -267,6 +267,45 @@ NNB_API NeonufftError nnb_plan_t3_geometry(NnbPrecision precision, int dim, cons
 NNB_API NeonufftError nnb_deconv_factors(double tol, double upsampfac, NnbPrecision precision,
                                          int64_t nf, double* out);
 
+/* ---------------------------------------------------------------------------------------
+ * Batched execution of many independent type-1 / type-2 transforms of uneven sizes.
+ * No counterpart in the reference, which runs one plan at a time; this is the engine's
+ * batch entry point (one plan per transform, spread over internal streams by estimated cost).
+ * ------------------------------------------------------------------------------------- */
+typedef struct NnbBatch_s* NnbBatch;
+
+typedef enum NnbBatchMode {
+  NNB_BATCH_SERIAL = 0,  /* one transform after the other */
+  NNB_BATCH_STREAMS = 1, /* the internal streams run concurrently */
+  NNB_BATCH_GRAPH = 2    /* the concurrent launch sequence captured once in a CUDA graph */
+} NnbBatchMode;
+
+/* Creates an empty batch with default options `opt` (NULL = defaults), num_streams in [1, 64]
+ * internal streams, forked from and joined into `stream`. */
+NNB_API NeonufftError nnb_batch_create(NnbBatch* batch, NnbPrecision precision,
+                                       const NnbOptions* opt, int num_streams, void* stream,
+                                       const NnbAllocator* alloc);
+
+/* Adds a type-1 (type = 1: in = strengths, out = modes with `strides`) or type-2 (type = 2:
+ * in = modes with `strides`, out = values at the points) transform and bins its points
+ * (synchronising its stream). `opt` overrides the batch options for this transform (NULL =
+ * the batch's). The input and output pointers are kept: every execution reads and writes the
+ * same buffers. *index receives the transform's index (may be NULL). */
+NNB_API NeonufftError nnb_batch_add(NnbBatch batch, int dim, int type, int sign, int64_t num_nu,
+                                    const void* const* loc, const int64_t* modes,
+                                    const void* in, void* out, const int64_t* strides,
+                                    const NnbOptions* opt, int64_t* index);
+
+/* Runs every transform of the batch on the batch stream (mode: NnbBatchMode). Asynchronous. */
+NNB_API NeonufftError nnb_batch_execute(NnbBatch batch, int mode);
+
+/* Number of transforms; information on transform `index`. */
+NNB_API NeonufftError nnb_batch_size(NnbBatch batch, int64_t* count);
+NNB_API NeonufftError nnb_batch_info(NnbBatch batch, int64_t index, NnbPlanInfo* info);
+
+/* Waits for the batch's work and frees it. */
+NNB_API NeonufftError nnb_batch_destroy(NnbBatch batch);
+
 /* Library version string. */
 NNB_API const char* nnb_version(void);
 

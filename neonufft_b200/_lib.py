@@ -16,6 +16,7 @@ SUCCESS, GENERIC_ERROR, MEMORY_ALLOC_ERROR, UNKNOWN_ERROR, INTERNAL_ERROR, INPUT
     GPU_ERROR, NOT_IMPLEMENTED_ERROR = range(8)
 
 NNB_FLOAT, NNB_DOUBLE = 0, 1
+NNB_BATCH_SERIAL, NNB_BATCH_STREAMS, NNB_BATCH_GRAPH = 0, 1, 2
 STAGES = ("bin", "spread", "fft", "deconv", "interp", "phase")
 
 
@@ -87,6 +88,12 @@ SIGNATURES = [
     ("nnb_es_kernel_params", _E, [C.c_double, C.c_double, C.c_int, C.POINTER(C.c_int), _PD, _PD]),
     ("nnb_plan_t3_geometry", _E, [C.c_int, C.c_int, C.POINTER(NnbOptions), _PD, _PD, _PD, _PD, _PI64, _PI64, _PD, _PD, _PD, _PD]),
     ("nnb_deconv_factors", _E, [C.c_double, C.c_double, C.c_int, _I64, _PD]),
+    ("nnb_batch_create", _E, [C.POINTER(_P), C.c_int, C.POINTER(NnbOptions), C.c_int, _P, C.POINTER(NnbAllocator)]),
+    ("nnb_batch_add", _E, [_P, C.c_int, C.c_int, C.c_int, _I64, _PP, _PI64, _P, _P, _PI64, C.POINTER(NnbOptions), _PI64]),
+    ("nnb_batch_execute", _E, [_P, C.c_int]),
+    ("nnb_batch_size", _E, [_P, _PI64]),
+    ("nnb_batch_info", _E, [_P, _I64, C.POINTER(NnbPlanInfo)]),
+    ("nnb_batch_destroy", _E, [_P]),
     ("nnb_version", C.c_char_p, []),
     ("nnb_kernel_launches", C.c_int64, []),
 ]

@@ -7,8 +7,12 @@
 
 #include "kernels.cuh"
 #include "neonufft_gpu.h"
+#include "batch.hpp"
 #include "plan.hpp"
 
+struct NnbBatch_s {
+  std::unique_ptr<nnb::Batch> impl;
+};
 struct NnbPlan_s {
   std::unique_ptr<nnb::PlanBase> impl;
 };
@@ -73,6 +77,57 @@ void nnb_options_default(NnbOptions* opt) {
 }
 
 const char* nnb_last_error_message(void) { return t_last_error.c_str(); }
+
+NeonufftError nnb_batch_create(NnbBatch* batch, NnbPrecision precision, const NnbOptions* opt,
+                               int num_streams, void* stream, const NnbAllocator* alloc) {
+  return guard([&] {
+    need(batch, "batch handle");
+    *batch = nullptr;
+    auto b = std::make_unique<NnbBatch_s>();
+    b->impl = std::make_unique<nnb::Batch>(precision, opts_or_default(opt), num_streams,
+                                           static_cast<cudaStream_t>(stream), alloc);
+    *batch = b.release();
+  });
+}
+
+NeonufftError nnb_batch_add(NnbBatch batch, int dim, int type, int sign, int64_t num_nu,
+                            const void* const* loc, const int64_t* modes, const void* in,
+                            void* out, const int64_t* strides, const NnbOptions* opt,
+                            int64_t* index) {
+  return guard([&] {
+    need(batch, "batch");
+    const int64_t i =
+        batch->impl->add(dim, type, sign, num_nu, loc, modes, in, out, strides, opt);
+    if (index) *index = i;
+  });
+}
+
+NeonufftError nnb_batch_execute(NnbBatch batch, int mode) {
+  return guard([&] {
+    need(batch, "batch");
+    batch->impl->execute(mode);
+  });
+}
+
+NeonufftError nnb_batch_size(NnbBatch batch, int64_t* count) {
+  return guard([&] {
+    need(batch, "batch");
+    need(count, "count");
+    *count = batch->impl->size();
+  });
+}
+
+NeonufftError nnb_batch_info(NnbBatch batch, int64_t index, NnbPlanInfo* info) {
+  return guard([&] {
+    need(batch, "batch");
+    need(info, "info");
+    batch->impl->plan(index).info(info);
+  });
+}
+
+NeonufftError nnb_batch_destroy(NnbBatch batch) {
+  return guard([&] { delete batch; });
+}
 
 const char* nnb_version(void) { return "neonufft_b200 0.1.0 (sm_100a)"; }
 

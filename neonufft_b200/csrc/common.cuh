@@ -139,11 +139,23 @@ struct alignas(16) PointRec {
 static_assert(sizeof(PointRec<float>) == 32 && sizeof(PointRec<double>) == 32,
               "point records are one 32-byte sector");
 
+// Device scratch of a point set for the kernels' work lists (worklist.cu).
+struct WorkScratch {
+  u32* cnt;       // items per unit (max_units)
+  u32* start;     // exclusive scan of cnt (max_units + 1)
+  u32* tmp;       // scan partials
+  u32* owner;     // unit of each item (max_items)
+  i64 max_units;
+  i64 max_items;
+};
+
 // Device-side view of a bin-sorted point set (records in tile order, length M).
 template <typename T>
 struct SortedPoints {
   const PointRec<T>* rec;
   const u32* bin_start;  // total_tiles + 1 offsets into the records
+  i64 M;
+  WorkScratch work;
 };
 
 // ES kernel (exponential of semicircle): phi(x) = exp(beta * (sqrt(1 - c x^2) - 1)) for

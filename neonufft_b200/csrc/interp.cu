@@ -53,7 +53,8 @@ __device__ __forceinline__ void stage_region(const BinGeom& g, const TileLayout&
 
 template <typename T, int DIM, int W>
 __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(InterpArgs<T> a,
-                                                                           TileLayout L) {
+                                                                           TileLayout L,
+                                                                           WorkList wl) {
   using C = cplx_t<T>;
   const int nwarps = blockDim.x >> 5;
   constexpr int KS = (DIM * W) | 1;
@@ -65,8 +66,10 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
   constexpr int LD = DIM - 1;
   const int n_last = g.ntiles[LD];
   const int groups = (n_last + nwarps - 1) / nwarps;
-  const i64 rest = blockIdx.x / groups;
-  const int grp = int(blockIdx.x - rest * groups);
+  u32 unit, slice;
+  if (!work_item(wl, unit, slice)) return;
+  const i64 rest = unit / groups;
+  const int grp = int(unit - rest * groups);
   int tc[3] = {0, 0, 0};
   {
     i64 r = rest;
@@ -87,11 +90,13 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
     if (DIM == 2) return tc[0] + i64(g.ntiles[0]) * t_last;
     return tc[0] + i64(g.ntiles[0]) * (tc[1] + i64(g.ntiles[1]) * t_last);
   };
-  // Skip CTAs without points (no staging traffic).
+  // This CTA's slice of each tile's points; skip CTAs without points (no staging traffic).
   bool any = false;
   for (int w = 0; w < nvalid; ++w) {
     const i64 b = bin_of(tc[LD] + w);
-    any |= a.pts.bin_start[b + 1] > a.pts.bin_start[b];
+    u32 s0, s1;
+    work_slice(a.pts.bin_start[b], a.pts.bin_start[b + 1], slice, wl.cap, s0, s1);
+    any |= s1 > s0;
   }
   if (!any) return;
 
@@ -105,8 +110,8 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
 
   if (warp >= nvalid) return;
   const i64 bin = bin_of(tc[LD] + warp);
-  const u32 start = a.pts.bin_start[bin];
-  const u32 end = a.pts.bin_start[bin + 1];
+  u32 start, end;
+  work_slice(a.pts.bin_start[bin], a.pts.bin_start[bin + 1], slice, wl.cap, start, end);
   T* kvb = kbuf + warp * 32 * KS;
   const int shift = warp * T_last * ((DIM == 3) ? L.PS : (DIM == 2 ? L.RS : 1));
 
@@ -202,14 +207,17 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
 
 // Thread-per-point variant on one staged tile per CTA.
 template <typename T, int DIM, int W>
-__global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a, TileLayout L) {
+__global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a, TileLayout L,
+                                                                  WorkList wl) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tile = reinterpret_cast<C*>(smem_raw);
   const BinGeom& g = a.g;
-  const i64 bin = blockIdx.x;
-  const u32 start = a.pts.bin_start[bin];
-  const u32 end = a.pts.bin_start[bin + 1];
+  u32 unit, slice;
+  if (!work_item(wl, unit, slice)) return;
+  const i64 bin = unit;
+  u32 start, end;
+  work_slice(a.pts.bin_start[bin], a.pts.bin_start[bin + 1], slice, wl.cap, start, end);
   if (start == end) return;
   const i64 t0 = bin % g.ntiles[0];
   const i64 t1 = DIM > 1 ? (bin / g.ntiles[0]) % g.ntiles[1] : 0;
@@ -265,7 +273,12 @@ void launch_interp_tw(const InterpArgs<T>& a, cudaStream_t stream) {
     if (smem > 227 * 1024) throw_internal("interpolation tile does not fit in shared memory");
     auto kern = interp_tpp_kernel<T, DIM, W>;
     NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kern<<<unsigned(a.g.total_tiles), kTppThreads, smem, stream>>>(a, L);
+    UnitMap m{};
+    m.kind = UnitMap::kTile;
+    m.units = a.g.total_tiles;
+    const WorkList wl = build_work_list(m, a.g, a.pts.bin_start, a.pts.M, a.pts.work, stream);
+    if (wl.grid > 0x7fffffffll) throw_input("grid too large");
+    kern<<<unsigned(wl.grid), kTppThreads, smem, stream>>>(a, L, wl);
     NNB_LAUNCH_CHECK();
     return;
   }
@@ -282,9 +295,14 @@ void launch_interp_tw(const InterpArgs<T>& a, cudaStream_t stream) {
   if (smem > 227 * 1024) throw_internal("interpolation tile does not fit in shared memory");
   auto kern = interp_slab_kernel<T, DIM, W>;
   NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  const i64 groups = (a.g.ntiles[LD] + nw - 1) / nw;
-  const i64 ctas = a.g.total_tiles / a.g.ntiles[LD] * groups;
-  kern<<<unsigned(ctas), nw * 32, smem, stream>>>(a, L);
+  UnitMap m{};
+  m.kind = UnitMap::kSlab;
+  m.nw = nw;
+  m.groups = (a.g.ntiles[LD] + nw - 1) / nw;
+  m.units = a.g.total_tiles / a.g.ntiles[LD] * m.groups;
+  const WorkList wl = build_work_list(m, a.g, a.pts.bin_start, a.pts.M, a.pts.work, stream);
+  if (wl.grid > 0x7fffffffll) throw_input("grid too large");
+  kern<<<unsigned(wl.grid), nw * 32, smem, stream>>>(a, L, wl);
   NNB_LAUNCH_CHECK();
 }
 

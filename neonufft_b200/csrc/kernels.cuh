@@ -24,6 +24,44 @@ template <typename T>
 void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
                         const u32* bin_start, PointRec<T>* rec, cudaStream_t stream);
 
+// ---- work lists (worklist.cu) ---------------------------------------------------------------
+// Launch units (one CTA each) split into items of at most kWorkItemPoints points.
+constexpr u32 kWorkItemPoints = 4096;
+struct UnitMap {
+  enum { kZwin = 0, kSlab = 1, kTile = 2 };
+  int kind;
+  i64 units;
+  i64 ncols;   // kZwin: columns; unit = chunk * ncols + column
+  int nz;      // kZwin: planes
+  int zlen;    // kZwin: planes per chunk
+  int nw;      // kSlab: tiles per unit along the last dimension
+  i64 groups;  // kSlab: units per row of tiles along the last dimension
+};
+struct WorkList {
+  const u32* owner;  // unit of each item
+  const u32* start;  // first item of each unit (units + 1)
+  i64 units;
+  u32 cap;           // points per item
+  i64 grid;          // CTAs to launch (an upper bound on the number of items)
+};
+WorkList build_work_list(const UnitMap& m, const BinGeom& g, const u32* bin_start, i64 M,
+                         const WorkScratch& s, cudaStream_t stream);
+// Unit and slice of the calling CTA's item (blockIdx.x); false if the CTA has no item.
+__device__ __forceinline__ bool work_item(const WorkList& wl, u32& unit, u32& slice) {
+  const u32 i = blockIdx.x;
+  if (i >= wl.start[wl.units]) return false;
+  unit = wl.owner[i];
+  slice = i - wl.start[unit];
+  return true;
+}
+// Points [begin, end) of slice `slice` of a bin's range [b0, b1).
+__device__ __forceinline__ void work_slice(u32 b0, u32 b1, u32 slice, u32 cap, u32& begin,
+                                           u32& end) {
+  const u64 s = u64(b0) + u64(slice) * cap;
+  begin = s < b1 ? u32(s) : b1;
+  end = (u64(begin) + cap) < b1 ? begin + cap : b1;
+}
+
 // ---- spreading (spread.cu) ------------------------------------------------------------------
 template <typename T>
 struct SpreadArgs {

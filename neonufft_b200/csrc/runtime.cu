@@ -195,7 +195,7 @@ template class FftGrid<double>;
 template <typename T>
 PointSet<T>::PointSet(std::shared_ptr<DeviceAllocator> alloc)
     : rec_(alloc), counts_(alloc), bin_start_(alloc), ranks_(alloc), scan_tmp_(alloc),
-      err_(alloc) {}
+      work_start_(alloc), work_owner_(alloc), err_(alloc) {}
 
 template <typename T>
 void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream) {
@@ -212,6 +212,9 @@ void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t st
   scan_tmp_.reserve(size_t(scan_tmp_words(nt)));
   rec_.reserve(size_t(M));
   ranks_.reserve(size_t(M));
+  // work lists reuse counts_ and scan_tmp_ after binning (launch units never exceed the tiles)
+  work_start_.reserve(size_t(nt + 1));
+  work_owner_.reserve(size_t(nt + M / kWorkItemPoints + 2));
   err_.reserve(1);
   NNB_CUDA(cudaMemsetAsync(counts_.data(), 0, sizeof(u32) * nt, stream));
   NNB_CUDA(cudaMemsetAsync(err_.data(), 0, sizeof(int), stream));
@@ -231,6 +234,13 @@ template <typename T>
 SortedPoints<T> PointSet<T>::view() const {
   SortedPoints<T> v;
   v.rec = rec_.data();
+  v.M = M_;
+  v.work.cnt = counts_.data();
+  v.work.start = work_start_.data();
+  v.work.tmp = scan_tmp_.data();
+  v.work.owner = work_owner_.data();
+  v.work.max_units = g_.total_tiles;
+  v.work.max_items = g_.total_tiles + M_ / kWorkItemPoints + 2;
   v.bin_start = bin_start_.data();
   return v;
 }

@@ -146,7 +146,7 @@ private:
   BinGeom g_{};
   i64 M_ = 0;
   DevArray<PointRec<T>> rec_;
-  DevArray<u32> counts_, bin_start_, ranks_, scan_tmp_;
+  DevArray<u32> counts_, bin_start_, ranks_, scan_tmp_, work_start_, work_owner_;
   DevArray<int> err_;
 };
 

@@ -70,7 +70,8 @@ __device__ __forceinline__ void writeback_rows(const BinGeom& g, const TileLayou
 
 template <typename T, int DIM, int W>
 __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadArgs<T> a,
-                                                                         TileLayout L) {
+                                                                         TileLayout L,
+                                                                         WorkList wl) {
   using C = cplx_t<T>;
   const int nwarps = blockDim.x >> 5;
   constexpr int KS = (DIM * W) | 1;  // odd stride: lanes write their rows without conflicts
@@ -82,8 +83,10 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
   constexpr int LD = DIM - 1;  // slabs are stacked along the last dimension
   const int n_last = g.ntiles[LD];
   const int groups = (n_last + nwarps - 1) / nwarps;
-  const i64 rest = blockIdx.x / groups;
-  const int grp = int(blockIdx.x - rest * groups);
+  u32 unit, slice;
+  if (!work_item(wl, unit, slice)) return;
+  const i64 rest = unit / groups;
+  const int grp = int(unit - rest * groups);
   int tc[3] = {0, 0, 0};  // tile coordinates of warp 0
   {
     i64 r = rest;
@@ -105,11 +108,13 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
     if (DIM == 2) return tc[0] + i64(g.ntiles[0]) * t_last;
     return tc[0] + i64(g.ntiles[0]) * (tc[1] + i64(g.ntiles[1]) * t_last);
   };
-  // CTAs without points contribute nothing.
+  // This CTA's slice of each tile's points; CTAs without points contribute nothing.
   bool any = false;
   for (int w = 0; w < nvalid; ++w) {
     const i64 b = bin_of(tc[LD] + w);
-    any |= a.pts.bin_start[b + 1] > a.pts.bin_start[b];
+    u32 s0, s1;
+    work_slice(a.pts.bin_start[b], a.pts.bin_start[b + 1], slice, wl.cap, s0, s1);
+    any |= s1 > s0;
   }
   if (!any) return;
 
@@ -120,8 +125,8 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
   const int warp = threadIdx.x >> 5;
   if (warp < nvalid) {
     const i64 bin = bin_of(tc[LD] + warp);
-    const u32 start = a.pts.bin_start[bin];
-    const u32 end = a.pts.bin_start[bin + 1];
+    u32 start, end;
+    work_slice(a.pts.bin_start[bin], a.pts.bin_start[bin + 1], slice, wl.cap, start, end);
     C* slab = slabs + warp * L.cells;
     T* kvb = kbuf + warp * 32 * KS;
 
@@ -295,13 +300,16 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
 
 // Thread-per-point variant with shared-memory atomics on one padded tile per CTA.
 template <typename T, int DIM, int W>
-__global__ void __launch_bounds__(kTppThreads) spread_tpp_kernel(SpreadArgs<T> a, TileLayout L) {
+__global__ void __launch_bounds__(kTppThreads) spread_tpp_kernel(SpreadArgs<T> a, TileLayout L,
+                                                                  WorkList wl) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const BinGeom& g = a.g;
-  const i64 bin = blockIdx.x;
-  const u32 start = a.pts.bin_start[bin];
-  const u32 end = a.pts.bin_start[bin + 1];
+  u32 unit, slice;
+  if (!work_item(wl, unit, slice)) return;
+  const i64 bin = unit;
+  u32 start, end;
+  work_slice(a.pts.bin_start[bin], a.pts.bin_start[bin + 1], slice, wl.cap, start, end);
   if (start == end) return;
   C* acc = reinterpret_cast<C*>(smem_raw);
   T* accf = reinterpret_cast<T*>(smem_raw);
@@ -370,8 +378,13 @@ void launch_spread_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
     if (smem > 227 * 1024) throw_internal("spread tile does not fit in shared memory");
     auto kern = spread_tpp_kernel<T, DIM, W>;
     NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    dim3 grid(unsigned(a.g.total_tiles), unsigned(a.batch), 1);
-    kern<<<grid, kTppThreads, smem, stream>>>(a, L);
+    UnitMap m{};
+    m.kind = UnitMap::kTile;
+    m.units = a.g.total_tiles;
+    const WorkList wl = build_work_list(m, a.g, a.pts.bin_start, a.pts.M, a.pts.work, stream);
+    if (wl.grid > 0x7fffffffll) throw_input("grid too large");
+    dim3 grid(unsigned(wl.grid), unsigned(a.batch), 1);
+    kern<<<grid, kTppThreads, smem, stream>>>(a, L, wl);
     NNB_LAUNCH_CHECK();
     return;
   }
@@ -386,10 +399,15 @@ void launch_spread_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
   // Per device and cheap; set on every launch so that multi-device processes stay correct.
   NNB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int LD = DIM - 1;
-  const i64 groups = (a.g.ntiles[LD] + nw - 1) / nw;
-  const i64 ctas = a.g.total_tiles / a.g.ntiles[LD] * groups;
-  dim3 grid(unsigned(ctas), unsigned(a.batch), 1);
-  kern<<<grid, nw * 32, smem, stream>>>(a, L);
+  UnitMap m{};
+  m.kind = UnitMap::kSlab;
+  m.nw = nw;
+  m.groups = (a.g.ntiles[LD] + nw - 1) / nw;
+  m.units = a.g.total_tiles / a.g.ntiles[LD] * m.groups;
+  const WorkList wl = build_work_list(m, a.g, a.pts.bin_start, a.pts.M, a.pts.work, stream);
+  if (wl.grid > 0x7fffffffll) throw_input("grid too large");
+  dim3 grid(unsigned(wl.grid), unsigned(a.batch), 1);
+  kern<<<grid, nw * 32, smem, stream>>>(a, L, wl);
   NNB_LAUNCH_CHECK();
 }
 

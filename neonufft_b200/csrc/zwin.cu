@@ -204,20 +204,20 @@ struct ZCta {
   u32 pbeg, pend;
 };
 __device__ __forceinline__ bool zcta(const BinGeom& g, const u32* bin_start, ZChunks ch,
-                                     ZCta& c) {
+                                     const WorkList& wl, ZCta& c) {
+  u32 unit, slice;
+  if (!work_item(wl, unit, slice)) return false;
   const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
-  const int chunk = int(blockIdx.x / ncols);
-  const i64 col = blockIdx.x - i64(chunk) * ncols;
+  const int chunk = int(unit / ncols);
+  const i64 col = unit - i64(chunk) * ncols;
   c.tx = int(col % g.ntiles[0]);
   c.ty = int(col / g.ntiles[0]);
   const int nz = g.ntiles[2];  // == nf[2]: single-plane tiles
   c.z0 = chunk * ch.len;
   c.z1 = min(c.z0 + ch.len, nz);
-  if (c.z0 >= c.z1) return false;
   const u32* bs = bin_start + col * nz;
-  c.pbeg = bs[c.z0];
-  c.pend = bs[c.z1];
-  return c.pbeg != c.pend;
+  work_slice(bs[c.z0], bs[c.z1], slice, wl.cap, c.pbeg, c.pend);
+  return c.pbeg < c.pend;
 }
 
 // Thread layout shared by both kernels.
@@ -244,7 +244,7 @@ struct ZThread {
 // ---- spreading ---------------------------------------------------------------------------------
 template <typename T, int W, int TX>
 __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
-    spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch) {
+    spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch, WorkList wl) {
   using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
 
   const BinGeom& g = a.g;
   ZCta cta;
-  if (!zcta(g, a.pts.bin_start, ch, cta)) return;
+  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
   const ZThread<T, W, TX> th;
   const int batch = blockIdx.y;
   const C* in = a.in + batch * a.in_bdist;
@@ -362,7 +362,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 template <typename T, int W, int TX>
 __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
-    interp_zwin_kernel(InterpArgs<T> a, ZChunks ch) {
+    interp_zwin_kernel(InterpArgs<T> a, ZChunks ch, WorkList wl) {
   using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
 
   const BinGeom& g = a.g;
   ZCta cta;
-  if (!zcta(g, a.pts.bin_start, ch, cta)) return;
+  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
   const ZThread<T, W, TX> th;
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
@@ -574,15 +574,29 @@ ZChunks make_chunks(i64 ncols, int nz, int w) {
   return ch;
 }
 
+// Work list of (column, chunk) units split into items of at most kWorkItemPoints points.
+template <typename T>
+WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch,
+                        cudaStream_t stream) {
+  UnitMap m{};
+  m.kind = UnitMap::kZwin;
+  m.ncols = i64(g.ntiles[0]) * g.ntiles[1];
+  m.units = m.ncols * ch.count;
+  m.nz = g.ntiles[2];
+  m.zlen = ch.len;
+  const WorkList wl = build_work_list(m, g, pts.bin_start, pts.M, pts.work, stream);
+  if (wl.grid > 0x7fffffffll) throw_input("grid too large");
+  return wl;
+}
+
 template <typename T, int W, int TX>
 void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
   using S = ZShape<T, W, TX>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
-  const i64 ctas = ncols * ch.count;
-  if (ctas > 0x7fffffffll) throw_input("grid too large");
-  dim3 grid{unsigned(ctas), unsigned(a.batch), 1u};
-  spread_zwin_kernel<T, W, TX><<<grid, S::NT, 0, stream>>>(a, ch);
+  const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
+  dim3 grid{unsigned(wl.grid), unsigned(a.batch), 1u};
+  spread_zwin_kernel<T, W, TX><<<grid, S::NT, 0, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();
 }
 
@@ -591,9 +605,8 @@ void launch_interp_zwin_tw(const InterpArgs<T>& a, cudaStream_t stream) {
   using S = ZShape<T, W, TX>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
-  const i64 ctas = ncols * ch.count;
-  if (ctas > 0x7fffffffll) throw_input("grid too large");
-  interp_zwin_kernel<T, W, TX><<<unsigned(ctas), S::NT, 0, stream>>>(a, ch);
+  const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
+  interp_zwin_kernel<T, W, TX><<<unsigned(wl.grid), S::NT, 0, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();
 }
 

@@ -326,6 +326,66 @@ def _info_dict(i: L.NnbPlanInfo) -> dict:
     }
 
 
+class Batch:
+    """Many independent type-1 / type-2 transforms of uneven sizes run together (engine
+    extension, nnb_batch_* in include/neonufft_gpu.h): one plan per transform on internal streams,
+    executed serially, concurrently, or as one captured CUDA graph."""
+
+    SERIAL, STREAMS, GRAPH = L.NNB_BATCH_SERIAL, L.NNB_BATCH_STREAMS, L.NNB_BATCH_GRAPH
+
+    def __init__(self, opt: Options, dtype, num_streams: int = 4, stream=None,
+                 device_alloc=None):
+        lib = L.load()
+        self.precision = _precision(dtype, [])
+        self._stream = _stream(stream)
+        self._alloc = _Alloc(device_alloc) if device_alloc is not None else None
+        self._opt = opt if opt is not None else Options()
+        self._keep = []  # tensors whose pointers the batch holds
+        h = C.c_void_p()
+        c_opt = self._opt.to_c()
+        check(lib.nnb_batch_create(C.byref(h), self.precision, C.byref(c_opt), int(num_streams),
+                                   self._stream, C.byref(self._alloc.c) if self._alloc else None))
+        self._h = h
+
+    def add(self, type_: int, sign: int, loc: Sequence, modes: Sequence[int], inp, out,
+            strides: Sequence[int], opt: Options = None) -> int:
+        """Adds a transform; the batch keeps references to loc, inp and out."""
+        idx = C.c_int64(0)
+        c_opt = opt.to_c() if opt is not None else None
+        num_nu = int(loc[0].numel()) if hasattr(loc[0], "numel") else 0
+        check(L.load().nnb_batch_add(self._h, len(modes), int(type_), int(sign), num_nu,
+                                     L.ptr_array([_ptr(a) for a in loc]), L.i64_array(modes),
+                                     _ptr(inp), _ptr(out), L.i64_array(strides),
+                                     C.byref(c_opt) if c_opt is not None else None,
+                                     C.byref(idx)))
+        self._keep.append((loc, inp, out))
+        return idx.value
+
+    def execute(self, mode: int = GRAPH) -> None:
+        check(L.load().nnb_batch_execute(self._h, int(mode)))
+
+    def __len__(self) -> int:
+        n = C.c_int64(0)
+        check(L.load().nnb_batch_size(self._h, C.byref(n)))
+        return n.value
+
+    def info(self, index: int) -> dict:
+        i = L.NnbPlanInfo()
+        check(L.load().nnb_batch_info(self._h, int(index), C.byref(i)))
+        return _info_dict(i)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            L.load().nnb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---- FP64 direct sums on the GPU (accuracy measurement) -------------------------------------
 def direct_type1_f64(sign: int, loc: Sequence, c, modes_idx, out, stream=None) -> None:
     """out[s] = sum_j c[j] exp(i sign k_s . x_j); modes_idx is an int64 CUDA tensor (S, dim)."""

@@ -177,3 +177,26 @@ def test_type3_methods_batched(dtype, method, cuda, engine, oracle):
     for k in range(B):
         ref = oracle.direct_type3(1, p_in, c[k * M:(k + 1) * M], p_out)
         assert oracle.rel_l2(res[k * K:(k + 1) * K], ref) < bound
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+@pytest.mark.parametrize("dim,method", [(2, 1), (2, 2), (3, 1), (3, 2), (3, 3)])
+@pytest.mark.parametrize("type_", [1, 2])
+def test_heavy_tile_split_over_ctas(dtype, dim, method, type_, cuda, engine, oracle):
+    """12000 points inside one tile: the tile's points are split into several work items of at
+    most 4096 points, each on its own CTA (partial grids added with atomics for spreading)."""
+    rng = np.random.default_rng(17 + dim + type_)
+    modes = [20, 18, 16][:dim]
+    M0, M1 = 12000, 200
+    pts = [np.concatenate([-1.0 + rng.uniform(0, 0.02, M0), rng.uniform(-np.pi, np.pi, M1)])
+           for _ in range(dim)]
+    M = M0 + M1
+    n_in = M if type_ == 1 else int(np.prod(modes))
+    inp = rng.standard_normal(n_in) + 1j * rng.standard_normal(n_in)
+    tol = 1e-5 if dtype == "float32" else 1e-7
+    out, info = run_t12(engine, cuda, dtype, -1, pts, inp, modes, type_, tol=tol,
+                        spread_method=method)
+    assert info["spread_method"] == method
+    ref = direct(oracle, type_, -1, pts, inp, modes, dtype)
+    # the bound of the reference matrix tests: max(10 tol, 2e-5) in single precision
+    assert oracle.rel_l2(out, ref) < (1e-4 if dtype == "float32" else 1e-6)
