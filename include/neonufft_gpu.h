@@ -306,6 +306,27 @@ NNB_API NeonufftError nnb_batch_info(NnbBatch batch, int64_t index, NnbPlanInfo*
 /* Waits for the batch's work and frees it. */
 NNB_API NeonufftError nnb_batch_destroy(NnbBatch batch);
 
+/* ---------------------------------------------------------------------------------------
+ * Multilayer perceptron of the learned cost model (FP32, device pointers, asynchronous on
+ * `stream`). No counterpart in the reference: the engine's tuner predicts run times of
+ * transform configurations with it. n_layers weight layers, widths[0..n_layers]; hidden layers
+ * tanh, output linear; parameters per layer: W (widths[l] x widths[l-1], row-major) then b.
+ * acts / dacts hold sum_{l>=1} widths[l] * batch floats (the output is the last block).
+ * ------------------------------------------------------------------------------------- */
+NNB_API NeonufftError nnb_mlp_param_count(int n_layers, const int* widths, int64_t* count);
+NNB_API NeonufftError nnb_mlp_forward(int n_layers, const int* widths, const float* params,
+                                      const float* x, int64_t batch, float* acts, void* stream);
+/* On entry the last block of dacts holds dLoss/dOutput; dacts is overwritten. */
+NNB_API NeonufftError nnb_mlp_backward(int n_layers, const int* widths, const float* params,
+                                       const float* x, const float* acts, float* dacts,
+                                       int64_t batch, float* grads, void* stream);
+/* dy = 2 (y - target) / n and loss = mean squared error (one float). */
+NNB_API NeonufftError nnb_mlp_mse(const float* y, const float* target, int64_t n, float* dy,
+                                  float* loss, void* stream);
+NNB_API NeonufftError nnb_mlp_adam(int64_t n, float* params, const float* grads, float* m,
+                                   float* v, float lr, float beta1, float beta2, float eps,
+                                   int64_t step, void* stream);
+
 /* Library version string. */
 NNB_API const char* nnb_version(void);
 

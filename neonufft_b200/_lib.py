@@ -94,6 +94,11 @@ SIGNATURES = [
     ("nnb_batch_size", _E, [_P, _PI64]),
     ("nnb_batch_info", _E, [_P, _I64, C.POINTER(NnbPlanInfo)]),
     ("nnb_batch_destroy", _E, [_P]),
+    ("nnb_mlp_param_count", _E, [C.c_int, C.POINTER(C.c_int), _PI64]),
+    ("nnb_mlp_forward", _E, [C.c_int, C.POINTER(C.c_int), _P, _P, _I64, _P, _P]),
+    ("nnb_mlp_backward", _E, [C.c_int, C.POINTER(C.c_int), _P, _P, _P, _P, _I64, _P, _P]),
+    ("nnb_mlp_mse", _E, [_P, _P, _I64, _P, _P, _P]),
+    ("nnb_mlp_adam", _E, [_I64, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P]),
     ("nnb_version", C.c_char_p, []),
     ("nnb_kernel_launches", C.c_int64, []),
 ]

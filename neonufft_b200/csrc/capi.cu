@@ -129,6 +129,61 @@ NeonufftError nnb_batch_destroy(NnbBatch batch) {
   return guard([&] { delete batch; });
 }
 
+NeonufftError nnb_mlp_param_count(int n_layers, const int* widths, int64_t* count) {
+  return guard([&] {
+    need(count, "count");
+    *count = nnb::mlp_param_count(n_layers, widths);
+  });
+}
+
+NeonufftError nnb_mlp_forward(int n_layers, const int* widths, const float* params,
+                              const float* x, int64_t batch, float* acts, void* stream) {
+  return guard([&] {
+    need(params, "params");
+    need(acts, "activations");
+    if (batch > 0) need(x, "inputs");
+    nnb::mlp_forward(n_layers, widths, params, x, batch, acts, static_cast<cudaStream_t>(stream));
+  });
+}
+
+NeonufftError nnb_mlp_backward(int n_layers, const int* widths, const float* params,
+                               const float* x, const float* acts, float* dacts, int64_t batch,
+                               float* grads, void* stream) {
+  return guard([&] {
+    need(params, "params");
+    need(acts, "activations");
+    need(dacts, "activation gradients");
+    need(grads, "gradients");
+    if (batch > 0) need(x, "inputs");
+    nnb::mlp_backward(n_layers, widths, params, x, acts, dacts, batch, grads,
+                      static_cast<cudaStream_t>(stream));
+  });
+}
+
+NeonufftError nnb_mlp_mse(const float* y, const float* target, int64_t n, float* dy, float* loss,
+                          void* stream) {
+  return guard([&] {
+    need(y, "outputs");
+    need(target, "targets");
+    need(dy, "output gradients");
+    need(loss, "loss");
+    nnb::mlp_mse(y, target, n, dy, loss, static_cast<cudaStream_t>(stream));
+  });
+}
+
+NeonufftError nnb_mlp_adam(int64_t n, float* params, const float* grads, float* m, float* v,
+                           float lr, float beta1, float beta2, float eps, int64_t step,
+                           void* stream) {
+  return guard([&] {
+    need(params, "params");
+    need(grads, "gradients");
+    need(m, "first moments");
+    need(v, "second moments");
+    nnb::mlp_adam(n, params, grads, m, v, lr, beta1, beta2, eps, step,
+                  static_cast<cudaStream_t>(stream));
+  });
+}
+
 const char* nnb_version(void) { return "neonufft_b200 0.1.0 (sm_100a)"; }
 
 int64_t nnb_kernel_launches(void) { return nnb::g_kernel_launches.load(); }

@@ -143,6 +143,17 @@ void launch_postphase(int dim, int sign, CoordPtrs<T> s, i64 K, const double* ou
                       const double* in_offset, const double* scale, const PostphaseQuad& q,
                       cplx_t<T>* post, cudaStream_t stream);
 
+// ---- MLP of the learned cost model (mlp.cu) --------------------------------------------------
+i64 mlp_param_count(int L, const int* widths);
+void mlp_forward(int L, const int* widths, const float* params, const float* x, i64 batch,
+                 float* acts, cudaStream_t stream);
+void mlp_backward(int L, const int* widths, const float* params, const float* x,
+                  const float* acts, float* dacts, i64 batch, float* grads, cudaStream_t stream);
+void mlp_mse(const float* y, const float* target, i64 n, float* dy, float* loss,
+             cudaStream_t stream);
+void mlp_adam(i64 n, float* params, const float* grads, float* m, float* v, float lr,
+              float beta1, float beta2, float eps, i64 step, cudaStream_t stream);
+
 // ---- FP64 direct sums (direct.cu) ------------------------------------------------------------
 void launch_direct_type1(int dim, int sign, i64 M, const double* const* loc, const double* in,
                          i64 S, const i64* modes_idx, double* out, cudaStream_t stream);

@@ -1,0 +1,232 @@
+"""Configuration tuning for the engine's plans: the plain heuristic, a measuring autotuner, and a
+learned picker.
+
+A configuration is (upsampling factor, kernel width, spreading method, tile). The plain
+heuristic is the reference's parameter choice (upsampfac 2, w from the tolerance,
+es_kernel_param.hpp:24-56) with the plan's default method and tile. The autotuner runs every
+candidate configuration of a problem on the GPU, measures its time and its error against the
+engine's FP64 direct sums on sampled outputs, and keeps the fastest one that meets the
+tolerance. The learned picker ranks the candidates with a cost model (costmodel.CostModel, an
+MLP trained on the autotuner's timings) and accepts the best-ranked candidate only once its
+measured error meets the tolerance, falling back to the heuristic otherwise. No counterpart in
+the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .plan import Options, Plan, check, direct_type1_f64, direct_type2_f64
+
+
+@dataclass(frozen=True)
+class Problem:
+    dim: int
+    type: int          # 1 or 2
+    M: int
+    N: int             # modes per dimension
+    tol: float
+    precision: str = "f32"
+    blob: bool = False  # points in a Gaussian blob (sigma 0.1) instead of uniform
+    seed: int = 0
+
+
+@dataclass(frozen=True)
+class Config:
+    upsampfac: float = 2.0
+    n_spread: int = 0        # 0: the reference heuristic for (tol, upsampfac)
+    method: int = 0          # 0: the plan's default
+    tile: tuple = (0, 0, 0)  # (0, 0, 0): the plan's default
+
+    def options(self, tol: float) -> Options:
+        return Options(tol=tol, upsampfac=self.upsampfac, n_spread=self.n_spread,
+                       spread_method=self.method, tile=self.tile)
+
+
+HEURISTIC = Config()
+
+
+def heuristic_width(tol: float, upsampfac: float, precision: str) -> int:
+    w, beta, c = C.c_int(0), C.c_double(0), C.c_double(0)
+    prec = L.NNB_DOUBLE if precision == "f64" else L.NNB_FLOAT
+    check(L.load().nnb_es_kernel_params(tol, upsampfac, prec, C.byref(w), C.byref(beta),
+                                        C.byref(c)))
+    return w.value
+
+
+def resolved(p: Problem, c: Config):
+    """(kernel width, method, x tile) that a plan with configuration c uses."""
+    w = c.n_spread or heuristic_width(p.tol, c.upsampfac, p.precision)
+    method = c.method or (3 if p.dim == 3 and w <= 8 else 1)
+    tile0 = c.tile[0] or ((8 if p.precision == "f32" else 4) if method == 3 else 0)
+    return w, method, tile0
+
+
+def candidates(p: Problem):
+    """The heuristic first, then every (upsampfac, width, method, tile) the tuner considers."""
+    out = [HEURISTIC]
+    for sigma in (2.0, 1.5):
+        w0 = heuristic_width(p.tol, sigma, p.precision)
+        for w in (w0, w0 + 1):
+            if w > 16:
+                continue
+            if p.dim == 3:
+                methods = [(1, (0, 0, 0))]
+                if w <= 8:
+                    methods = [(3, (8, 8, 1)), (3, (4, 8, 1))] + methods
+            elif p.dim == 2:
+                methods = [(1, (0, 0, 0)), (2, (0, 0, 0))]
+            else:
+                methods = [(1, (0, 0, 0))]
+            for m, tile in methods:
+                c = Config(sigma, w, m, tile)
+                if c not in out:
+                    out.append(c)
+    return out
+
+
+def features(p: Problem, c: Config) -> np.ndarray:
+    w, method, tile0 = resolved(p, c)
+    nf = max(2 * w, int(p.N * c.upsampfac))
+    lcells = p.dim * math.log10(nf)
+    return np.array([
+        float(p.dim == 3), float(p.type == 2), math.log10(p.M), p.dim * math.log10(p.N), lcells,
+        -math.log10(p.tol), float(p.precision == "f64"), float(p.blob), c.upsampfac, float(w),
+        float(method == 1), float(method == 2), float(method == 3), float(tile0),
+        math.log10(p.M) - lcells, float(w) ** p.dim / 100.0,
+    ], dtype=np.float64)
+
+
+N_FEATURES = 16
+
+
+class ProblemData:
+    """Seeded device inputs of a problem (points, strengths or modes, output buffer)."""
+
+    def __init__(self, p: Problem):
+        import torch
+        self.p = p
+        rdt = torch.float64 if p.precision == "f64" else torch.float32
+        cdt = torch.complex128 if p.precision == "f64" else torch.complex64
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1000 + p.seed)
+        if p.blob:
+            centre = (torch.rand(p.dim, generator=g, device="cuda", dtype=torch.float64) * 2 - 1) * math.pi
+            self.loc = [torch.remainder(centre[d] + 0.1 * torch.randn(p.M, generator=g, device="cuda",
+                                                                        dtype=torch.float64) + math.pi,
+                                        2 * math.pi).sub(math.pi).to(rdt) for d in range(p.dim)]
+        else:
+            self.loc = [((torch.rand(p.M, generator=g, device="cuda", dtype=torch.float64) * 2 - 1)
+                         * math.pi).to(rdt) for _ in range(p.dim)]
+        n_in = p.M if p.type == 1 else p.N ** p.dim
+        self.inp = torch.complex(torch.randn(n_in, generator=g, device="cuda", dtype=torch.float64),
+                                 torch.randn(n_in, generator=g, device="cuda", dtype=torch.float64)).to(cdt)
+        n_out = p.N ** p.dim if p.type == 1 else p.M
+        self.out = torch.empty(n_out, dtype=cdt, device="cuda")
+        self.strides = [p.N ** d for d in range(p.dim)]
+        self._ref = None
+
+    def reference(self, samples: int = 256):
+        """(indices, FP64 direct sums) on sampled outputs, computed once."""
+        import torch
+        if self._ref is None:
+            p = self.p
+            g = torch.Generator(device="cuda")
+            g.manual_seed(7)
+            loc64 = [a.double() for a in self.loc]
+            ref = torch.empty(samples, dtype=torch.complex128, device="cuda")
+            if p.type == 1:
+                idx = torch.randint(0, p.N ** p.dim, (samples,), generator=g, device="cuda")
+                kk, rem = [], idx.clone()
+                for _ in range(p.dim):
+                    kk.append(rem % p.N - p.N // 2)
+                    rem = rem // p.N
+                direct_type1_f64(-1, loc64, self.inp.to(torch.complex128),
+                                 torch.stack(kk, dim=1).contiguous(), ref)
+            else:
+                idx = torch.randint(0, p.M, (samples,), generator=g, device="cuda")
+                direct_type2_f64(-1, [p.N] * p.dim, self.inp.to(torch.complex128), loc64, idx, ref)
+            self._ref = (idx, ref)
+        return self._ref
+
+
+def measure(p: Problem, c: Config, data: ProblemData = None, reps: int = 3):
+    """(milliseconds per set_points + transform, relative l2 error on sampled outputs)."""
+    import torch
+    data = data or ProblemData(p)
+    plan = Plan(c.options(p.tol), -1, p.M, data.loc, [p.N] * p.dim)
+
+    def run():
+        plan.set_points(p.M, data.loc)
+        if p.type == 1:
+            plan.transform_type_1(data.inp, data.out, data.strides)
+        else:
+            plan.transform_type_2(data.inp, data.strides, data.out)
+
+    run()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    idx, ref = data.reference()
+    got = data.out[idx].to(torch.complex128)
+    err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+    plan.close()
+    return float(np.median(times)), err
+
+
+class Tuner:
+    """Heuristic, autotuner and learned picker over the candidates of a problem."""
+
+    def __init__(self, model=None):
+        self.model = model
+        self.rows = []  # (features, log10 ms, error, problem, config)
+
+    def sweep(self, problems):
+        """Measures every candidate of every problem (the autotuner's data and the model's)."""
+        for p in problems:
+            data = ProblemData(p)
+            for c in candidates(p):
+                ms, err = measure(p, c, data)
+                self.rows.append((features(p, c), math.log10(ms), err, p, c))
+        return self.rows
+
+    def autotune(self, p: Problem):
+        """Fastest measured candidate of p meeting its tolerance (from the sweep rows)."""
+        best = None
+        for f, lms, err, q, c in self.rows:
+            if q == p and err <= p.tol and (best is None or lms < best[0]):
+                best = (lms, c)
+        return best[1] if best else HEURISTIC
+
+    def train(self, rows=None, epochs: int = 3000, seed: int = 0) -> float:
+        from .costmodel import CostModel
+        rows = rows if rows is not None else self.rows
+        feats = np.stack([r[0] for r in rows])
+        y = np.array([r[1] for r in rows])
+        self.model = CostModel(feats.shape[1], seed=seed)
+        return self.model.fit(feats, y, epochs=epochs)
+
+    def pick(self, p: Problem, data: ProblemData = None):
+        """(configuration, measured (ms, error), candidates tried): the best-ranked candidate
+        whose measured error meets tol; the heuristic when none does."""
+        cands = candidates(p)
+        if self.model is None:
+            return HEURISTIC, None, 0
+        pred = self.model.predict(np.stack([features(p, c) for c in cands]))
+        data = data or ProblemData(p)
+        for tried, i in enumerate(np.argsort(pred), start=1):
+            ms, err = measure(p, cands[int(i)], data)
+            if err <= p.tol:
+                return cands[int(i)], (ms, err), tried
+        return HEURISTIC, measure(p, HEURISTIC, data), len(cands)

@@ -123,3 +123,23 @@ def test_acceptance_rule_rejects_planted_error(oracle):
     bad[7] *= 1.01  # squared relative error 1e-4 > 400 * tol
     assert not oracle.reference_compare(ref, bad, 1e-8, 400, 0.85)[0]
     assert oracle.rel_l2(bad, ref) > 10 * oracle.rel_l2(out, ref)
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The cost-model oracle's analytic gradient against central differences (float64)."""
+    from oracle import mlp_oracle as MO
+    rng = np.random.default_rng(3)
+    widths = [5, 7, 6, 1]
+    p = rng.standard_normal(MO.param_count(widths)) * 0.5
+    x = rng.standard_normal((11, 5))
+    t = rng.standard_normal(11)
+
+    def loss(params):
+        return MO.mse(MO.forward(widths, params, x)[-1], t)[0]
+
+    acts = MO.forward(widths, p, x)
+    _, dy = MO.mse(acts[-1], t)
+    g = MO.backward(widths, p, x, acts, dy.reshape(-1, 1))
+    h = 1e-6
+    fd = np.array([(loss(p + h * e) - loss(p - h * e)) / (2 * h) for e in np.eye(p.size)])
+    assert np.max(np.abs(fd - g)) < 1e-7 * max(1.0, np.max(np.abs(g)))
