@@ -45,6 +45,14 @@ WORKLOADS = {
     "c4": dict(name="64 uneven 2D/3D type-1 transforms in one batch, M log-uniform [1e4,1e7], "
                     "N per dim in {64,128,256,512} (3D <= 256), half Gaussian blobs (sigma 0.1), tol 1e-6",
                batch=64, tol=1e-6, types=(1,), seed=4, tuned_w=8),
+    "c5": dict(name="tuner sweep: 60 seeded problems, dim {2,3}, type {1,2}, M log-uniform "
+                    "[1e5,1e7], N per dim 64-256 (3D <= 128), tol {1e-3,1e-6} FP32 and 1e-9 FP64, "
+                    "uniform or blobs; MLP trained on 40, picks scored on 20 against the heuristic",
+               tuner=60, train=40, seed=5),
+    "c3": dict(name="type 3, M=K=5e6, sources uniform in a box of half-width 50, targets in "
+                    "half-width 200, tol 1e-5: 2D at the literal extents (the 3D grids need "
+                    "~1.5e14 B), 3D at half-widths 9 and 36",
+               t3=True, M=5_000_000, X=50.0, S=200.0, X3=9.0, S3=36.0, tol=1e-5, seed=3),
     "c1": dict(name="2D type-1, M=1e5 uniform [-pi,pi)^2, N=256^2, tol 1e-6",
                dim=2, M=100_000, N=256, tol=1e-6, types=(1,), seed=1, cpu_sample=100_000,
                tuned_w=8),
@@ -366,6 +374,160 @@ def run_batch(args, wl):
     return 0
 
 
+def run_tuner(args, wl):
+    """Learned-tuner workload: sweep, train the cost model, score its picks on held-out problems
+    against the plain heuristic (time where the heuristic meets tol, and tol compliance)."""
+    import numpy as np
+    import torch
+    from neonufft_b200 import tuner as T
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(wl["seed"] + 97 * rank)
+    problems = []
+    for i in range(wl["tuner"]):
+        dim = int(rng.choice([2, 3]))
+        f64 = i % 5 == 4
+        N = int(rng.choice([64, 96, 128] if dim == 3 else [64, 128, 256]))
+        problems.append(T.Problem(dim=dim, type=int(rng.choice([1, 2])),
+                                  M=int(10 ** rng.uniform(5, 7)), N=N,
+                                  tol=1e-9 if f64 else float(rng.choice([1e-3, 1e-6])),
+                                  precision="f64" if f64 else "f32", blob=bool(rng.random() < 0.5),
+                                  seed=i))
+    train, held = problems[:wl["train"]], problems[wl["train"]:]
+    tuner = T.Tuner()
+    t0 = time.perf_counter()
+    tuner.sweep(train)
+    sweep_s = time.perf_counter() - t0
+    loss = tuner.train(epochs=3000)
+    pts_pick = ms_pick = pts_heur = ms_heur = 0.0
+    ratios, ratios_all, best_ratio, heur_fail, tried, heur_err = [], [], [], 0, [], []
+    for p in held:
+        data = T.ProblemData(p)
+        cfg, (ms, err), k = tuner.pick(p, data)
+        h_ms, h_err = T.measure(p, T.HEURISTIC, data)
+        tried.append(k)
+        heur_err.append(h_err / p.tol)
+        pts_pick += p.M
+        ms_pick += ms
+        ratios_all.append(h_ms / ms)
+        if h_err <= p.tol:
+            ratios.append(h_ms / ms)
+            pts_heur += p.M
+            ms_heur += h_ms
+        else:
+            heur_fail += 1
+        # the exhaustive autotuner's best candidate meeting tol, for comparison
+        best = min((T.measure(p, c, data) for c in T.candidates(p)),
+                   key=lambda r: r[0] if r[1] <= p.tol else float("inf"))
+        if best[1] <= p.tol:
+            best_ratio.append(best[0] / ms)
+
+    def geo(v):
+        return float(np.exp(np.mean(np.log(v)))) if v else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": pts_pick / (ms_pick * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": 1, "warmup": 1, "ms_per_step": ms_pick / max(1, len(held)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+            "data": "synthetic (seeded problems; uniform or Gaussian-blob points)",
+            "config": {"workload": wl["name"], "train_problems": len(train),
+                       "held_out": len(held), "sweep_s": sweep_s, "train_loss": loss},
+            "tuner": {"speedup_vs_heuristic_geomean_where_it_meets_tol": geo(ratios),
+                      "time_ratio_heuristic_over_pick_geomean_all": geo(ratios_all),
+                      "heuristic_missed_tol": heur_fail,
+                      "heuristic_error_over_tol_median": float(np.median(heur_err)),
+                      "picks_meeting_tol": len(held),
+                      "pick_time_over_autotuner_best_geomean": (1.0 / geo(best_ratio)
+                                                                 if best_ratio else None),
+                      "candidates_measured_per_pick": float(np.mean(tried)),
+                      "heuristic_points_per_s": (pts_heur / (ms_heur * 1e-3)) if ms_heur else None},
+            "e2e": None, "gpu_launches": None, "roofline": None, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_type3(args, wl):
+    """Type-3 workload: the literal 3D extents are checked for memory only; 2D runs at the
+    literal extents and 3D at reduced ones (same 1:4 ratio)."""
+    import numpy as np
+    import torch
+    import neonufft_b200 as nnb
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    M, tol = wl["M"], wl["tol"]
+    # the reference heuristic width (w = 6 at tol 1e-5) misses tol 1e-5 for type 3 (two kernel
+    # passes); the tuned width is one larger unless --n-spread says otherwise
+    n_spread = args.n_spread if args.n_spread >= 0 else 7
+    opt = nnb.Options(tol=tol, n_spread=n_spread)
+    X, S = wl["X"], wl["S"]
+    bytes3 = nnb.PlanT3.grid_memory_size(opt, [-X] * 3, [X] * 3, [-S] * 3, [S] * 3,
+                                         dtype=torch.float32)
+    cases = {}
+    for dim, (x, s_) in ((2, (X, S)), (3, (wl["X3"], wl["S3"]))):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(wl["seed"] + 97 * rank + dim)
+        xin = [(torch.rand(M, generator=g, device="cuda") * 2 - 1) * x for _ in range(dim)]
+        xout = [(torch.rand(M, generator=g, device="cuda") * 2 - 1) * s_ for _ in range(dim)]
+        c = torch.complex(torch.randn(M, generator=g, device="cuda"),
+                          torch.randn(M, generator=g, device="cuda"))
+        out = torch.empty(M, dtype=torch.complex64, device="cuda")
+        plan = nnb.PlanT3(opt, -1, M, xin, M, xout)
+        info = plan.info()
+
+        def step():
+            plan.set_input_points(M, xin)
+            plan.set_output_points(M, xout)
+            plan.reset()
+            plan.add_input(c)
+            plan.transform(out)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        acc = None
+        if not args.no_accuracy:
+            gs = torch.Generator(device="cuda")
+            gs.manual_seed(123)
+            idx = torch.randint(0, M, (2000,), generator=gs, device="cuda")
+            ref = torch.empty(2000, dtype=torch.complex128, device="cuda")
+            nnb.direct_type3_f64(-1, [a.double() for a in xin], c.to(torch.complex128),
+                                 [a.double() for a in xout], idx, ref)
+            got = out[idx].to(torch.complex128)
+            acc = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        cases[f"{dim}d"] = {"ms_per_step": ms, "points_per_s": M / (ms * 1e-3),
+                            "rel_l2": acc, "spread_grid": info["spread_grid"][:dim],
+                            "fft_grid": info["grid"][:dim], "n_spread": info["n_spread"],
+                            "half_widths": [x, s_]}
+        plan.close()
+        del xin, xout, c, out
+        torch.cuda.empty_cache()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": cases["2d"]["points_per_s"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cases["2d"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform sources and targets, N(0,1) strengths)",
+            "config": {"workload": wl["name"], "M": M, "K": M, "tol": tol,
+                       "literal_3d_grid_bytes": int(bytes3), "literal_3d": "infeasible",
+                       "step": "set_input_points + set_output_points + reset + add_input + transform"},
+            "cases": cases, "e2e": None, "gpu_launches": None, "roofline": None,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,13 +551,17 @@ def main():
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
-        if "batch" in wl:
+        if "batch" in wl or "tuner" in wl or "t3" in wl:
             print(json.dumps({"impl": "reference", "unavailable":
-                              "the batched workload has no CPU reference arm"}))
+                              "this workload has no CPU reference arm"}))
             return 0
         return run_reference(args, wl)
     if "batch" in wl:
         return run_batch(args, wl)
+    if "tuner" in wl:
+        return run_tuner(args, wl)
+    if "t3" in wl:
+        return run_type3(args, wl)
 
     import numpy as np
     import torch
