@@ -553,6 +553,7 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
     ap.add_argument("--streams", type=int, default=8, help="internal streams of a batch (c4)")
+    ap.add_argument("--upsampfac", type=float, default=2.0, help="upsampling factor sigma")
     ap.add_argument("--tile", default="",
                     help="engine tile shape, e.g. 4,8,1 (default: the plan's choice)")
     ap.add_argument("--n-spread", type=int, default=-1,
@@ -611,7 +612,8 @@ def main():
     # rel-l2 (even in FP64); the tuned width w = 8 meets rel-l2 <= 1e-6, the metric's bar.
     n_spread = wl.get("tuned_w", 0) if args.n_spread < 0 else args.n_spread
     tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 0, 0)
-    opt = nnb.Options(tol=tol, spread_method=args.spread_method, n_spread=n_spread, tile=tile)
+    opt = nnb.Options(tol=tol, upsampfac=args.upsampfac, spread_method=args.spread_method,
+                      n_spread=n_spread, tile=tile)
     plan = nnb.Plan(opt, -1, M, loc, modes)
     info = plan.info()
 
@@ -786,7 +788,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic (seeded uniform points, N(0,1) strengths and modes)",
             "config": {"workload": wl["name"], "M": M, "N": N, "dim": dim, "tol": tol,
-                       "upsampfac": 2.0, "n_spread": w, "fine_grid": info["grid"][:dim],
+                       "upsampfac": args.upsampfac, "n_spread": w, "fine_grid": info["grid"][:dim],
                        "tile": info["tile"][:dim], "method": info["spread_method"],
                        "precision": args.precision,
                        "parallelism": f"replicas x{world}",

@@ -198,6 +198,24 @@ __device__ __forceinline__ i64 wrap_x(i64 gx0, int i, i64 nfx, bool narrow) {
   return x;
 }
 
+// Plane p (p >= 0, below nfz plus a window) wrapped into the grid.
+__device__ __forceinline__ i64 wrap_plane(int p, i64 nfz) {
+  i64 z = p;
+  while (z >= nfz) z -= nfz;
+  return z;
+}
+
+// Adds two neighbouring cells (re0, im0), (re1, im1) at a 16-byte aligned address.
+__device__ __forceinline__ void atomic_add_pair(float2* p, float re0, float im0, float re1,
+                                                float im1) {
+  atomicAdd(reinterpret_cast<float4*>(p), make_float4(re0, im0, re1, im1));
+}
+__device__ __forceinline__ void atomic_add_pair(double2* p, double re0, double im0, double re1,
+                                                double im1) {
+  atomic_add_cplx(p, double2{re0, im0});
+  atomic_add_cplx(p + 1, double2{re1, im1});
+}
+
 // CTA coordinates: column (tx, ty), plane range [z0, z1) and its run of points [pbeg, pend).
 struct ZCta {
   int tx, ty, z0, z1;
@@ -271,17 +289,36 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   bool dirty = false;
 
   // Adds this thread's row of plane p (absolute; may exceed nfz) to the grid and clears it.
+  // The region's x range lies inside the grid and its rows start 16-byte aligned (the usual
+  // case): whole cell pairs are added with one vector atomic each.
+  const bool pairs = !narrow && gx0 + S::P0 <= nfx && (nfx % 2) == 0 &&
+                     (reinterpret_cast<size_t>(grid) % 16) == 0;
   auto flush = [&](int p) {
     if (has_row && dirty) {
-      C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
+      C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+      if (pairs) {
+        C* r = row + gx0;
 #pragma unroll
-      for (int q = 0; q < S::NP; ++q) {
-        atomic_add_cplx(&row[wrap_x(gx0, 2 * q, nfx, narrow)], C{Ops::lo(are[q]), Ops::lo(aim[q])});
-        if (2 * q + 1 < S::P0) {
-          atomic_add_cplx(&row[wrap_x(gx0, 2 * q + 1, nfx, narrow)],
-                          C{Ops::hi(are[q]), Ops::hi(aim[q])});
+        for (int q = 0; q < S::NP; ++q) {
+          if (2 * q + 1 < S::P0) {
+            atomic_add_pair(r + 2 * q, Ops::lo(are[q]), Ops::lo(aim[q]), Ops::hi(are[q]),
+                            Ops::hi(aim[q]));
+          } else {
+            atomic_add_cplx(r + 2 * q, C{Ops::lo(are[q]), Ops::lo(aim[q])});
+          }
+          are[q] = aim[q] = Ops::zero();
         }
-        are[q] = aim[q] = Ops::zero();
+      } else {
+#pragma unroll
+        for (int q = 0; q < S::NP; ++q) {
+          atomic_add_cplx(&row[wrap_x(gx0, 2 * q, nfx, narrow)],
+                          C{Ops::lo(are[q]), Ops::lo(aim[q])});
+          if (2 * q + 1 < S::P0) {
+            atomic_add_cplx(&row[wrap_x(gx0, 2 * q + 1, nfx, narrow)],
+                            C{Ops::hi(are[q]), Ops::hi(aim[q])});
+          }
+          are[q] = aim[q] = Ops::zero();
+        }
       }
     }
     dirty = false;
@@ -357,6 +394,10 @@ __device__ __forceinline__ void cp_async_cell(void* smem, const double2* g) {
   const unsigned s = unsigned(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(g) : "memory");
 }
+__device__ __forceinline__ void cp_async_16(void* smem, const void* g) {
+  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(g) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
@@ -394,14 +435,22 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   P gre[S::NP], gim[S::NP];
 #pragma unroll
   for (int q = 0; q < S::NP; ++q) gre[q] = gim[q] = Ops::zero();
+  // The region's x range lies inside the grid (the usual case): contiguous row segments.
+  const bool contiguous = !narrow && gx0 + S::P0 <= nfx;
+  const bool pairs16 = contiguous && (nfx % 2) == 0 && (reinterpret_cast<size_t>(grid) % 16) == 0;
   auto load_row = [&](int p) {
     if (!has_row) return;
-    const C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
+    const C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
 #pragma unroll
     for (int q = 0; q < S::NP; ++q) {
-      const C c0 = row[wrap_x(gx0, 2 * q, nfx, narrow)];
-      C c1{T(0), T(0)};
-      if (2 * q + 1 < S::P0) c1 = row[wrap_x(gx0, 2 * q + 1, nfx, narrow)];
+      C c0, c1{T(0), T(0)};
+      if (contiguous) {
+        c0 = row[gx0 + 2 * q];
+        if (2 * q + 1 < S::P0) c1 = row[gx0 + 2 * q + 1];
+      } else {
+        c0 = row[wrap_x(gx0, 2 * q, nfx, narrow)];
+        if (2 * q + 1 < S::P0) c1 = row[wrap_x(gx0, 2 * q + 1, nfx, narrow)];
+      }
       gre[q] = Ops::pack(c0.x, c1.x);
       gim[q] = Ops::pack(c0.y, c1.y);
     }
@@ -409,10 +458,22 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   bool pending = false;  // a cp.async of this thread's next plane is in flight
   auto prefetch = [&](int p) {
     if (!has_row) return;
-    const C* row = grid + ((i64(p) % nfz) * nfy + row_y) * nfx;
+    const C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+    if (pairs16 && sizeof(T) == 4) {
+      // 16-byte copies of cell pairs (the stage rows are 16-byte aligned)
 #pragma unroll
-    for (int i = 0; i < S::P0; ++i) {
-      cp_async_cell(&stage_row[th.ra][i], row + wrap_x(gx0, i, nfx, narrow));
+      for (int q = 0; q < S::NP; ++q) {
+        if (2 * q + 1 < S::P0) {
+          cp_async_16(&stage_row[th.ra][2 * q], row + gx0 + 2 * q);
+        } else {
+          cp_async_cell(&stage_row[th.ra][2 * q], row + gx0 + 2 * q);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < S::P0; ++i) {
+        cp_async_cell(&stage_row[th.ra][i], row + wrap_x(gx0, i, nfx, narrow));
+      }
     }
     cp_async_commit();
     pending = true;
