@@ -150,28 +150,68 @@ template <typename T, int W, int TX>
 struct alignas(16) ZSlot
     : ZSlotFields<T, W, TX>, ZSlotPad<(sizeof(ZSlotFields<T, W, TX>) / 16) % 2 == 1> {};
 
-// Stages bin-sorted record `rec` (plane-major packing) into slot `sl`.
-template <typename T, int W, int TX>
-__device__ __forceinline__ void stage_point(ZSlot<T, W, TX>& sl, const PointRec<T>& rec,
-                                            cplx_t<T> v, T beta, T c) {
+// Stages `count` (<= 16) bin-sorted records `recs` into slots[0 .. count), one warp: lanes
+// 0 .. count - 1 load the records (and, for spreading, the strengths); then lane pair
+// (2p, 2p + 1) fills point p's slot with the same instruction stream: the even lane kx and the
+// first half of kz, the odd lane ky and the second half, each zeroing half of the contiguous
+// kx / ky arrays first, so all 32 lanes evaluate kernel values.
+template <typename T, int W, int TX, bool SPREAD>
+__device__ __forceinline__ void stage_warp(ZSlot<T, W, TX>* slots, const PointRec<T>* recs,
+                                           int count, const cplx_t<T>* in,
+                                           const cplx_t<T>* prephase, T beta, T c, int lane) {
   using S = ZShape<T, W, TX>;
-  const u32 loc = rec.local;
-  const int lx = int(loc & 0xFu);
-  const int ly = int((loc >> 4) & 0xFu);
-  float4* z = reinterpret_cast<float4*>(sl.kx);  // kx and ky are contiguous, 16-byte multiples
-#pragma unroll
-  for (int i = 0; i < int((S::KXN + S::RY) * sizeof(T) / 16); ++i) z[i] = make_float4(0, 0, 0, 0);
-#pragma unroll
-  for (int k = 0; k < W; ++k) sl.kx[lx + k] = es_eval_fast<T>(rec.frac[0] + T(k), beta, c);
-#pragma unroll
-  for (int k = 0; k < W; ++k) sl.ky[ly + k] = es_eval_fast<T>(rec.frac[1] + T(k), beta, c);
-#pragma unroll
-  for (int k = 0; k < S::RZ; ++k) {
-    sl.kz[k] = k < W ? es_eval_fast<T>(rec.frac[2] + T(k), beta, c) : T(0);
+  using C = cplx_t<T>;
+  constexpr unsigned kFull = 0xffffffffu;
+  PointRec<T> rec;
+  rec.perm = 0;
+  rec.local = 0;
+  rec.frac[0] = rec.frac[1] = rec.frac[2] = T(0);
+  C v{T(0), T(0)};
+  if (lane < count) {
+    rec = recs[lane];
+    if constexpr (SPREAD) {
+      v = in[rec.perm];
+      if (prephase) v = cmul(v, prephase[rec.perm]);
+    }
   }
-  sl.v = v;
-  sl.lyp = ly | int((loc >> 8) << 4);
-  sl.perm = rec.perm;
+  const int p = lane >> 1;
+  const int h = lane & 1;
+  const u32 loc = __shfl_sync(kFull, rec.local, p);
+  const u32 perm = __shfl_sync(kFull, rec.perm, p);
+  const T fx = __shfl_sync(kFull, rec.frac[0], p);
+  const T fy = __shfl_sync(kFull, rec.frac[1], p);
+  const T fz = __shfl_sync(kFull, rec.frac[2], p);
+  const T vx = __shfl_sync(kFull, v.x, p);
+  const T vy = __shfl_sync(kFull, v.y, p);
+  ZSlot<T, W, TX>& sl = slots[p < count ? p : 0];
+  constexpr int kZero16 = int((S::KXN + S::RY) * sizeof(T) / 16);  // kx and ky are contiguous
+  constexpr int kHalf = (kZero16 + 1) / 2;
+  if (p < count) {
+    float4* z = reinterpret_cast<float4*>(sl.kx);
+#pragma unroll
+    for (int i = 0; i < kHalf; ++i) {
+      if (h * kHalf + i < kZero16) z[h * kHalf + i] = make_float4(0, 0, 0, 0);
+    }
+  }
+  __syncwarp();
+  if (p < count) {
+    const int lx = int(loc & 0xFu);
+    const int ly = int((loc >> 4) & 0xFu);
+    T* dst = h ? sl.ky + ly : sl.kx + lx;
+    const T f = h ? fy : fx;
+#pragma unroll
+    for (int k = 0; k < W; ++k) dst[k] = es_eval_fast<T>(f + T(k), beta, c);
+#pragma unroll
+    for (int i = 0; i < S::RZ / 2; ++i) {
+      const int k = h * (S::RZ / 2) + i;
+      sl.kz[k] = k < W ? es_eval_fast<T>(fz + T(k), beta, c) : T(0);
+    }
+    if (h == 0) {
+      sl.v = C{vx, vy};
+      sl.lyp = ly | int((loc >> 8) << 4);
+      sl.perm = perm;
+    }
+  }
 }
 
 // Chunk of planes handled by one CTA.
@@ -329,11 +369,12 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   auto stage = [&](int k) {
     const u32 off = u32(k) * S::BATCH;
     const int nb = int(min(npts - off, u32(S::BATCH)));
-    if (th.stage_j >= 0 && th.stage_j < nb) {
-      const PointRec<T> rec = a.pts.rec[cta.pbeg + off + th.stage_j];
-      C v = in[rec.perm];
-      if (a.prephase) v = cmul(v, a.prephase[rec.perm]);
-      stage_point<T, W, TX>(slots[k & 1][th.stage_j], rec, v, a.beta, a.c);
+    constexpr int PW = S::BATCH / S::NWARP;  // points per warp
+    const int count = min(nb - th.warp * PW, PW);
+    for (int c0 = 0; c0 < count; c0 += 16) {
+      stage_warp<T, W, TX, true>(slots[k & 1] + th.warp * PW + c0,
+                                 a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
+                                 min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane);
     }
   };
 
@@ -495,9 +536,12 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   auto stage = [&](int k) {
     const u32 off = u32(k) * S::BATCH;
     const int nb = int(min(npts - off, u32(S::BATCH)));
-    if (th.stage_j >= 0 && th.stage_j < nb) {
-      stage_point<T, W, TX>(slots[k & 1][th.stage_j], a.pts.rec[cta.pbeg + off + th.stage_j],
-                            C{T(0), T(0)}, a.beta, a.c);
+    constexpr int PW = S::BATCH / S::NWARP;  // points per warp
+    const int count = min(nb - th.warp * PW, PW);
+    for (int c0 = 0; c0 < count; c0 += 16) {
+      stage_warp<T, W, TX, false>(slots[k & 1] + th.warp * PW + c0,
+                                  a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
+                                  min(count - c0, 16), nullptr, nullptr, a.beta, a.c, th.lane);
     }
   };
   // Writes the outputs of batch k: this thread's staged point, whose slot only this thread's
