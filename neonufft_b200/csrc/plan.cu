@@ -58,7 +58,7 @@ void validate_options(const NnbOptions& opt) {
   for (int d = 0; d < 3; ++d) {
     if (opt.tile[d] < 0) throw_input("invalid tile shape");
   }
-  if (opt.spread_method < 0 || opt.spread_method > 3) throw_input("invalid spread method");
+  if (opt.spread_method < 0 || opt.spread_method > 4) throw_input("invalid spread method");
   if (opt.n_spread != 0 && (opt.n_spread < 2 || opt.n_spread > 16)) {
     throw_input("kernel width must be in [2, 16]");
   }
@@ -89,7 +89,7 @@ public:
     }
     kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
-    method_ = choose_method(dim, kp_.w, opt.spread_method);
+    method_ = choose_method(dim, kp_.w, opt.spread_method, is_single<T>());
     for (int d = 0; d < dim; ++d) nf_[d] = fine_grid_size(modes_[d], opt.upsampfac, kp_.w);
     fft_ = std::make_unique<FftGrid<T>>(alloc_, dim, nf_, sign_, stream_);
     for (int d = 0; d < dim; ++d) {
@@ -97,7 +97,7 @@ public:
       upload(corr_[d], deconv_factors(kp_, nf_[d]), stream_);
     }
     choose_tile(dim, kp_.w, sizeof(cplx_t<T>), nf_, opt.tile, method_, tile_);
-    geom_ = make_geom(dim, kp_.w, nf_, tile_, nullptr, nullptr, method_ == 3);
+    geom_ = make_geom(dim, kp_.w, nf_, tile_, nullptr, nullptr, method_ >= 3);
     set_points(M, loc);
   }
 
@@ -247,7 +247,7 @@ public:
     if (batch > 65535) throw_input("batch size above 65535");
     kp_ = kernel_param(opt.tol, opt.upsampfac, is_single<T>(), opt.n_spread);
     if (kp_.w < 2 || kp_.w > 16) throw_internal("n_spread not in [2, 16]");
-    method_ = choose_method(dim, kp_.w, opt.spread_method);
+    method_ = choose_method(dim, kp_.w, opt.spread_method, is_single<T>());
     for (auto& c : corr_) c.set_allocator(alloc_);
   }
 
@@ -352,7 +352,7 @@ public:
     }
     double scale[3];
     for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? 1.0 / gamma_[d] : 1.0;
-    const BinGeom g = make_geom(dim_, kp_.w, nf1_, in_tile_, C_, scale, method_ == 3);
+    const BinGeom g = make_geom(dim_, kp_.w, nf1_, in_tile_, C_, scale, method_ >= 3);
     ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
     in_points_.build(g, x, M, stream_);
   }
@@ -363,7 +363,7 @@ public:
     const CoordPtrs<T> s = coords<T>(dim_, pts);
     double scale[3];
     for (int d = 0; d < 3; ++d) scale[d] = d < dim_ ? gamma_[d] * h_[d] : 1.0;
-    const BinGeom g = make_geom(dim_, kp_.w, nfft_, out_tile_, D_, scale, method_ == 3);
+    const BinGeom g = make_geom(dim_, kp_.w, nfft_, out_tile_, D_, scale, method_ >= 3);
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_BIN);
       out_points_.build(g, s, K, stream_);

@@ -249,9 +249,12 @@ template class PointSet<float>;
 template class PointSet<double>;
 
 // ---- tiles ----------------------------------------------------------------------------------------
-int choose_method(int dim, int w, int requested) {
+int choose_method(int dim, int w, int requested, bool single) {
   if (requested == 3 && (dim != 3 || w > 8)) {
     throw_input("spread method 3 needs a 3D plan with kernel width <= 8");
+  }
+  if (requested == 4 && (dim != 3 || w < 5 || w > 8 || !single)) {
+    throw_input("spread method 4 needs a single-precision 3D plan with kernel width in [5, 8]");
   }
   if (requested > 0) return requested;
   return (dim == 3 && w <= 8) ? 3 : 1;
@@ -262,6 +265,13 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
   const int max_bits[3] = {dim == 3 ? 11 : (dim == 2 ? 16 : 31), dim == 3 ? 11 : 16, 10};
   bool explicit_tile = requested && requested[0] > 0;
   for (int d = 0; d < 3; ++d) tile[d] = 1;
+  if (method == 4) {
+    if (explicit_tile && requested[0] != 8) throw_input("spread method 4 uses tiles of 8 x 8 x 1");
+    tile[0] = 8;
+    tile[1] = 8;
+    tile[2] = 1;
+    return;
+  }
   if (method == 3) {
     // x tile of 8 cells for single precision (15-cell register rows at w = 8), 4 for double.
     tile[0] = complex_bytes == 8 ? 8 : 4;

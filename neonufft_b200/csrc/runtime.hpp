@@ -151,8 +151,9 @@ private:
 };
 
 // Spreading / interpolation method for a plan: the requested one (validated), or the default:
-// 3 (z-window, zwin.cu) for 3D plans with n_spread <= 8, else 1 (shared-memory slabs).
-int choose_method(int dim, int w, int requested);
+// 3 (z-window, zwin.cu) for 3D plans with n_spread <= 8, else 1 (shared-memory slabs). Method 4
+// is the z-window with tensor-core spreading (single precision, 5 <= n_spread <= 8).
+int choose_method(int dim, int w, int requested, bool single);
 
 // Tile shape for a grid and method: explicit request (validated) or the automatic choice.
 // Method 3 uses (tx, 8, 1) tiles, tx in {4, 8}.

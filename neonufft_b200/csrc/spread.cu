@@ -445,7 +445,7 @@ size_t spread_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, 
 template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream) {
   if (a.g.total_tiles <= 0 || a.batch <= 0) return;
-  if (a.method == 3) return launch_spread_zwin<T>(a, stream);
+  if (a.method == 3 || a.method == 4) return launch_spread_zwin<T>(a, stream);
   switch (a.g.dim) {
     case 1: return launch_spread_d<T, 1>(a, stream);
     case 2: return launch_spread_d<T, 2>(a, stream);

@@ -426,6 +426,181 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   flush(cur + ((th.rb - cur) & (S::RZ - 1)));  // the rest of the window
 }
 
+// ---- spreading on the tensor cores (method 4, single precision, 5 <= w <= 8) ---------------------
+//
+// The same window, staging and flushes as spread_zwin_kernel, with the per-point row updates
+// replaced by TF32 tensor-core products. For a chunk of up to 8 points of the current plane,
+//   region[x, (plane, y)] += sum_p kx_p[x] * (v_p ky_p[y] kz_p[plane])
+// is, for each tile of one plane and 8 rows, a 16 x 8 x 8 matrix product (mma.sync m16n8k8:
+// M = the 16 x cells of the region, K = the points, N = the rows). Both operands are split into
+// a TF32 value and a TF32 remainder and the product accumulated as hi*hi + hi*lo + lo*hi in FP32
+// (about 2^-21 of each product). Warp w owns window planes 2w, 2w + 1 (mod 8) and both 8-row y
+// groups: four tiles, real and imaginary accumulators in registers; in the m16n8k8 fragment
+// layout thread (q, t) = (lane / 4, lane % 4) holds x = q, q + 8 and rows 2t, 2t + 1 of a tile.
+// A completed plane is added to the grid by its owning warp (all 32 lanes, float2 atomics).
+
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+// c += a * b for one m16n8k8 TF32 tile (FP32 accumulation)
+__device__ __forceinline__ void mma_tf32(float* c, const unsigned* a, unsigned b0, unsigned b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// c += a * b with both operands split (3 products). The products of one chunk are summed on the
+// tensor core into a fresh tile and added to the accumulator with ordinary FP32 adds: chaining
+// the accumulator through every MMA of a long run of points loses accuracy.
+__device__ __forceinline__ void mma_tf32x3(float* c, const unsigned* ahi, const unsigned* alo,
+                                           float b0, float b1) {
+  unsigned b0h, b0l, b1h, b1l;
+  tf32_split(b0, b0h, b0l);
+  tf32_split(b1, b1h, b1l);
+  float t[4] = {0.f, 0.f, 0.f, 0.f};
+  mma_tf32(t, alo, b0h, b1h);
+  mma_tf32(t, ahi, b0l, b1l);
+  mma_tf32(t, ahi, b0h, b1h);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) c[e] += t[e];
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) spread_zmma_kernel(SpreadArgs<float> a, ZChunks ch,
+                                                          WorkList wl) {
+  constexpr int TX = 8;
+  using S = ZShape<float, W, TX>;
+  static_assert(S::RZ == 8 && S::NWARP == 4 && S::P0 <= 16, "tile shapes");
+  using C = float2;
+  using Slot = ZSlot<float, W, TX>;
+  __shared__ Slot slots[2][S::BATCH];
+
+  const BinGeom& g = a.g;
+  ZCta cta;
+  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
+  const ZThread<float, W, TX> th;
+  const int gq = th.lane >> 2;  // fragment row group
+  const int tq = th.lane & 3;   // thread in group
+  const bool hi8 = gq + 8 < S::KXN;  // staged kx covers x = gq + 8 (cells beyond it are zero)
+  const int batch = blockIdx.y;
+  const C* in = a.in + batch * a.in_bdist;
+  C* grid = a.grid + batch * a.grid_bdist;
+  const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
+  const bool narrow = nfx < S::P0;
+  const i64 gx0 = i64(cta.tx) * TX;
+  const i64 gy0 = i64(cta.ty) * S::TY;
+
+  float cre[2][2][4], cim[2][2][4];  // [plane of the warp][y group][fragment element]
+#pragma unroll
+  for (int pl = 0; pl < 2; ++pl) {
+#pragma unroll
+    for (int yg = 0; yg < 2; ++yg) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) cre[pl][yg][e] = cim[pl][yg][e] = 0.f;
+    }
+  }
+  unsigned dirty = 0;  // plane residues with contributions since their last flush
+
+  // Adds the warp's tiles of window plane p (residue 2 warp + pl) to the grid and clears them.
+  auto flush = [&](int pl, int p) {
+    const unsigned bit = 1u << (2 * th.warp + pl);
+    if (dirty & bit) {
+      const i64 plane = wrap_plane(p, nfz);
+#pragma unroll
+      for (int yg = 0; yg < 2; ++yg) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int x = gq + 8 * (e >> 1);
+          const int y = 8 * yg + 2 * tq + (e & 1);
+          if (x < S::P0 && y < S::P1) {
+            const i64 gy = wrap_add(gy0, y, nfy);
+            atomic_add_cplx(&grid[(plane * nfy + gy) * nfx + wrap_x(gx0, x, nfx, narrow)],
+                            C{cre[pl][yg][e], cim[pl][yg][e]});
+          }
+          cre[pl][yg][e] = cim[pl][yg][e] = 0.f;
+        }
+      }
+      dirty &= ~bit;
+    }
+  };
+  auto flush_plane = [&](int p) {
+    const int b = p & 7;
+    if ((b >> 1) == th.warp) flush(b & 1, p);
+  };
+
+  const u32 npts = cta.pend - cta.pbeg;
+  const int nbatch = int((npts + S::BATCH - 1) / S::BATCH);
+  auto stage = [&](int k) {
+    const u32 off = u32(k) * S::BATCH;
+    const int nb = int(min(npts - off, u32(S::BATCH)));
+    constexpr int PW = S::BATCH / S::NWARP;
+    const int count = min(nb - th.warp * PW, PW);
+    for (int c0 = 0; c0 < count; c0 += 16) {
+      stage_warp<float, W, TX, true>(slots[k & 1] + th.warp * PW + c0,
+                                     a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
+                                     min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane);
+    }
+  };
+
+  stage(0);
+  __syncthreads();
+  int cur = slots[0][0].lyp >> 4;
+  int dz0 = (2 * th.warp - cur) & 7, dz1 = (2 * th.warp + 1 - cur) & 7;
+  for (int k = 0; k < nbatch; ++k) {
+    const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
+    const Slot* sb = slots[k & 1];
+    int j = 0;
+    while (j < nb) {
+      const int tp = sb[j].lyp >> 4;
+      if (tp != cur) {  // advance the window: planes [cur, tp) are complete
+        const int n = min(tp - cur, S::RZ);
+        for (int i = 0; i < n; ++i) flush_plane(cur + i);
+        cur = tp;
+        dz0 = (2 * th.warp - cur) & 7;
+        dz1 = (2 * th.warp + 1 - cur) & 7;
+      }
+      // the chunk: points j .. j + n - 1 of plane cur (a prefix, the points are plane-sorted)
+      const bool on = th.lane < 8 && j + th.lane < nb && (sb[min(j + th.lane, nb - 1)].lyp >> 4) == cur;
+      const int n = __popc(__ballot_sync(0xffffffffu, on));
+      const bool h0 = tq < n, h1 = tq + 4 < n;
+      const Slot& s0 = sb[h0 ? j + tq : j];
+      const Slot& s1 = sb[h1 ? j + tq + 4 : j];
+      // A: kx of points tq, tq + 4 at x = gq, gq + 8
+      unsigned ahi[4], alo[4];
+      tf32_split(h0 ? s0.kx[gq] : 0.f, ahi[0], alo[0]);
+      tf32_split(h0 && hi8 ? s0.kx[gq + 8] : 0.f, ahi[1], alo[1]);
+      tf32_split(h1 ? s1.kx[gq] : 0.f, ahi[2], alo[2]);
+      tf32_split(h1 && hi8 ? s1.kx[gq + 8] : 0.f, ahi[3], alo[3]);
+      // B: v ky kz of points tq, tq + 4 at row gq of each tile
+      const C v0 = h0 ? s0.v : C{0.f, 0.f};
+      const C v1 = h1 ? s1.v : C{0.f, 0.f};
+      const float y00 = s0.ky[gq], y01 = s0.ky[gq + 8], z00 = s0.kz[dz0], z01 = s0.kz[dz1];
+      const float y10 = s1.ky[gq], y11 = s1.ky[gq + 8], z10 = s1.kz[dz0], z11 = s1.kz[dz1];
+#pragma unroll
+      for (int pl = 0; pl < 2; ++pl) {
+#pragma unroll
+        for (int yg = 0; yg < 2; ++yg) {
+          const float w0 = (yg ? y01 : y00) * (pl ? z01 : z00);
+          const float w1 = (yg ? y11 : y10) * (pl ? z11 : z10);
+          mma_tf32x3(cre[pl][yg], ahi, alo, v0.x * w0, v1.x * w1);
+          mma_tf32x3(cim[pl][yg], ahi, alo, v0.y * w0, v1.y * w1);
+        }
+      }
+      dirty = 0xffu;
+      j += n;
+    }
+    if (k + 1 < nbatch) stage(k + 1);
+    __syncthreads();
+  }
+  for (int i = 0; i < S::RZ; ++i) flush_plane(cur + i);  // the rest of the window
+}
+
 // ---- interpolation -----------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async_cell(void* smem, const float2* g) {
   const unsigned s = unsigned(__cvta_generic_to_shared(smem));
@@ -752,10 +927,33 @@ void check_zwin_geom(const BinGeom& g) {
 
 }  // namespace
 
+template <int W>
+void launch_spread_zmma_w(const SpreadArgs<float>& a, cudaStream_t stream) {
+  const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
+  const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
+  const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
+  dim3 grid{unsigned(wl.grid), unsigned(a.batch), 1u};
+  spread_zmma_kernel<W><<<grid, 128, 0, stream>>>(a, ch, wl);
+  NNB_LAUNCH_CHECK();
+}
+
 template <typename T>
 void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream) {
   check_zwin_geom(a.g);
   if (a.batch > 65535) throw_input("batch size above 65535");
+  if (a.method == 4) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.g.tile[0] != 8) throw_internal("tensor-core spreading needs tiles of 8 cells in x");
+      switch (a.g.w) {
+        case 5: return launch_spread_zmma_w<5>(a, stream);
+        case 6: return launch_spread_zmma_w<6>(a, stream);
+        case 7: return launch_spread_zmma_w<7>(a, stream);
+        case 8: return launch_spread_zmma_w<8>(a, stream);
+        default: throw_internal("tensor-core spreading needs 5 <= n_spread <= 8");
+      }
+    }
+    throw_internal("tensor-core spreading is single precision");
+  }
   if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8>(a, stream);
   return spread_zwin_tx<T, 4>(a, stream);
 }

@@ -200,3 +200,62 @@ def test_heavy_tile_split_over_ctas(dtype, dim, method, type_, cuda, engine, ora
     ref = direct(oracle, type_, -1, pts, inp, modes, dtype)
     # the bound of the reference matrix tests: max(10 tol, 2e-5) in single precision
     assert oracle.rel_l2(out, ref) < (1e-4 if dtype == "float32" else 1e-6)
+
+
+@pytest.mark.parametrize("w", [5, 6, 7, 8])
+@pytest.mark.parametrize("case", ["uniform", "tiny", "clustered"])
+def test_tensor_core_spreading_matches_zwin_and_direct(w, case, cuda, engine, oracle):
+    """Method 4 (z-window with TF32 tensor-core spreading, operands split into value and
+    remainder) against method 3 and the FP64 direct sum, FP32 type 1."""
+    rng = np.random.default_rng(60 + w)
+    if case == "tiny":
+        modes = [3, 2, 4]  # fine grid 2w: the region wraps around the grid
+        pts = [rng.uniform(-4, 4, 300) for _ in range(3)]
+    elif case == "clustered":  # one column chunk of ~9000 points: split over CTAs
+        modes = [20, 18, 16]
+        pts = [np.concatenate([0.5 + rng.uniform(0, 0.02, 9000), rng.uniform(-np.pi, np.pi, 300)])
+               for _ in range(3)]
+    else:
+        modes = [20, 17, 12]
+        pts = [rng.uniform(-np.pi, np.pi, 4000) for _ in range(3)]
+    M = len(pts[0])
+    c = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    out4, info4 = run_t12(engine, cuda, "float32", -1, pts, c, modes, 1, n_spread=w,
+                          spread_method=4)
+    out3, _ = run_t12(engine, cuda, "float32", -1, pts, c, modes, 1, n_spread=w, spread_method=3)
+    assert info4["spread_method"] == 4
+    ref = direct(oracle, 1, -1, pts, c, modes, "float32")
+    assert oracle.rel_l2(out4, ref) < width_bound("float32", w)
+    assert oracle.rel_l2(out4, out3) < 2e-6
+
+
+def test_tensor_core_spreading_type3_batched(cuda, engine, oracle):
+    import torch
+    rng = np.random.default_rng(70)
+    M, K, B = 900, 400, 2
+    xin = [rng.uniform(-3, 5, M).astype(np.float32) for _ in range(3)]
+    xout = [rng.uniform(-20, 12, K).astype(np.float32) for _ in range(3)]
+    c = rng.standard_normal(M * B) + 1j * rng.standard_normal(M * B)
+    plan = engine.PlanT3(engine.Options(tol=1e-5, spread_method=4), 1, M,
+                         [torch.from_numpy(p).cuda() for p in xin], K,
+                         [torch.from_numpy(p).cuda() for p in xout], batch_size=B)
+    out = torch.zeros(K * B, dtype=torch.complex64, device="cuda")
+    plan.add_input(torch.from_numpy(c.astype(np.complex64)).cuda(), M)
+    plan.transform(out, K)
+    torch.cuda.synchronize()
+    res = out.cpu().numpy()
+    plan.close()
+    for k in range(B):
+        ref = oracle.direct_type3(1, [p.astype(np.float64) for p in xin], c[k * M:(k + 1) * M],
+                                  [p.astype(np.float64) for p in xout])
+        assert oracle.rel_l2(res[k * K:(k + 1) * K], ref) < 5e-5
+
+
+def test_method4_rejected_outside_its_domain(cuda, engine):
+    import torch
+    loc3 = [torch.zeros(4, device="cuda") for _ in range(3)]
+    with pytest.raises(engine.InputError):
+        engine.Plan(engine.Options(tol=1e-3, spread_method=4), -1, 4, loc3, [8, 8, 8])  # w = 4
+    loc64 = [torch.zeros(4, device="cuda", dtype=torch.float64) for _ in range(3)]
+    with pytest.raises(engine.InputError):
+        engine.Plan(engine.Options(tol=1e-6, spread_method=4), -1, 4, loc64, [8, 8, 8])
