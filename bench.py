@@ -169,10 +169,24 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from neonufft_b200 import replicas
+    env = replicas.rank_env()
+    return env.world, env.rank, env.local
+
+
+def rank_seed(wl, rank):
+    from neonufft_b200 import replicas
+    return replicas.rank_seed(wl["seed"], rank)
+
+
+def max_over_ranks(ms):
+    from neonufft_b200 import replicas
+    return replicas.max_over_ranks(ms, "cuda")
+
+
+def job_throughput(world, units_per_rank, ms_per_step):
+    from neonufft_b200 import replicas
+    return replicas.job_throughput(world, units_per_rank, ms_per_step)
 
 
 def cpu_port_step(wl, M, workers):
@@ -228,7 +242,7 @@ def run_reference(args, wl):
 def batch_problems(wl, rank):
     """The seeded problems of the batched workload (host arrays)."""
     import numpy as np
-    rng = np.random.default_rng(wl["seed"] + 97 * rank)
+    rng = np.random.default_rng(rank_seed(wl, rank))
     probs = []
     for i in range(wl["batch"]):
         dim = 2 if i % 2 == 0 else 3
@@ -286,12 +300,7 @@ def run_batch(args, wl):
             batch.execute(mode)
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
     ms_serial = timed(nnb.Batch.SERIAL)
     l0 = nnb.kernel_launches()
@@ -327,7 +336,7 @@ def run_batch(args, wl):
         e2e()
     e1.record()
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / args.steps
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
     acc = {}
     if not args.no_accuracy:
@@ -352,7 +361,7 @@ def run_batch(args, wl):
                "samples_each": 2000}
     if rank == 0:
         line = {
-            "metric": METRIC, "value": world * total / (ms_graph * 1e-3), "unit": UNIT,
+            "metric": METRIC, "value": job_throughput(world, total, ms_graph), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded uniform and Gaussian-blob points, N(0,1) strengths)",
@@ -362,7 +371,7 @@ def run_batch(args, wl):
                        "l2": "inputs larger than L2 (126 MB); no flush"},
             "modes_ms_per_step": {"serial": ms_serial, "streams": ms_streams, "graph": ms_graph},
             "clocks": clk,
-            "e2e": {"value": world * total / (ms_e2e * 1e-3), "unit": UNIT,
+            "e2e": {"value": job_throughput(world, total, ms_e2e), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
             "gpu_launches": int(launches), "roofline": None, "cpu_baseline": None,
             "accuracy": acc,
@@ -383,7 +392,7 @@ def run_tuner(args, wl):
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    rng = np.random.default_rng(wl["seed"] + 97 * rank)
+    rng = np.random.default_rng(rank_seed(wl, rank))
     problems = []
     for i in range(wl["tuner"]):
         dim = int(rng.choice([2, 3]))
@@ -474,7 +483,7 @@ def run_type3(args, wl):
             w = args.n_spread
         opt = nnb.Options(tol=tol, n_spread=w)
         g = torch.Generator(device="cuda")
-        g.manual_seed(wl["seed"] + 97 * rank + dim)
+        g.manual_seed(rank_seed(wl, rank) + dim)
         rdt = torch.float64 if prec == "f64" else torch.float32
         xin = [(torch.rand(M, generator=g, device="cuda", dtype=rdt) * 2 - 1) * x
                for _ in range(dim)]
@@ -592,7 +601,7 @@ def main():
 
     dim, M, N, tol = wl["dim"], wl["M"], wl["N"], wl["tol"]
     g = torch.Generator(device="cuda")
-    g.manual_seed(wl["seed"] + 97 * rank)
+    g.manual_seed(rank_seed(wl, rank))
     f64 = args.precision == "f64"
     rdt = torch.float64 if f64 else torch.float32
     cdt = torch.complex128 if f64 else torch.complex64
@@ -649,14 +658,10 @@ def main():
     launches = nnb.kernel_launches() - l0
     stages = plan.stage_times(reset=True)
     plan.enable_timing(False)
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1))
     ms_step = ms / args.steps
     ntr = len(wl["types"])
-    value = world * ntr * M / (ms_step * 1e-3)
+    value = job_throughput(world, ntr * M, ms_step)
 
     # ---- end-to-end through the public API with host buffers --------------------------------
     pin = dict(device="cpu", pin_memory=True)
@@ -699,12 +704,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     barrier()
-    ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * ntr * M / (ms_e2e / args.steps * 1e-3)
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = job_throughput(world, ntr * M, ms_e2e / args.steps)
 
     # ---- accuracy vs the FP64 direct sum on sampled outputs (not timed) ---------------------
     acc = {}
