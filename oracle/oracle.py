@@ -512,6 +512,17 @@ class Ref:
                                     C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p]
         L.ref_gpu_type3.restype = C.c_int
+        L.ref_plan12_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_double,
+                                        C.c_double, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+        L.ref_plan12_create.restype = C.c_int
+        L.ref_plan12_set_points.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        L.ref_plan12_set_points.restype = C.c_int
+        L.ref_plan12_t1.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_plan12_t1.restype = C.c_int
+        L.ref_plan12_t2.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_plan12_t2.restype = C.c_int
+        L.ref_plan12_destroy.argtypes = [C.c_void_p]
+        L.ref_plan12_destroy.restype = None
         self.L = L
 
     def kernel_param(self, tol, upsampfac, single):
