@@ -275,9 +275,13 @@ NNB_API NeonufftError nnb_deconv_factors(double tol, double upsampfac, NnbPrecis
 typedef struct NnbBatch_s* NnbBatch;
 
 typedef enum NnbBatchMode {
-  NNB_BATCH_SERIAL = 0,  /* one transform after the other */
-  NNB_BATCH_STREAMS = 1, /* the internal streams run concurrently */
-  NNB_BATCH_GRAPH = 2    /* the concurrent launch sequence captured once in a CUDA graph */
+  NNB_BATCH_SERIAL = 0,      /* one transform after the other */
+  NNB_BATCH_STREAMS = 1,     /* the internal streams run concurrently */
+  NNB_BATCH_GRAPH = 2,       /* the concurrent launch sequence captured once in a CUDA graph */
+  NNB_BATCH_FUSED = 3,       /* as STREAMS, but the z-window spreading (type 1) and interpolation
+                                (type 2) steps of all 3D transforms that share a kernel shape run
+                                as one persistent launch over a queue of all their work items */
+  NNB_BATCH_FUSED_GRAPH = 4  /* FUSED captured once in a CUDA graph */
 } NnbBatchMode;
 
 /* Creates an empty batch with default options `opt` (NULL = defaults), num_streams in [1, 64]

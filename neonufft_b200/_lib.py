@@ -17,6 +17,7 @@ SUCCESS, GENERIC_ERROR, MEMORY_ALLOC_ERROR, UNKNOWN_ERROR, INTERNAL_ERROR, INPUT
 
 NNB_FLOAT, NNB_DOUBLE = 0, 1
 NNB_BATCH_SERIAL, NNB_BATCH_STREAMS, NNB_BATCH_GRAPH = 0, 1, 2
+NNB_BATCH_FUSED, NNB_BATCH_FUSED_GRAPH = 3, 4
 STAGES = ("bin", "spread", "fft", "deconv", "interp", "phase")
 
 

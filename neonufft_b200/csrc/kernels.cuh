@@ -46,13 +46,18 @@ struct WorkList {
 };
 WorkList build_work_list(const UnitMap& m, const BinGeom& g, const u32* bin_start, i64 M,
                          const WorkScratch& s, cudaStream_t stream);
-// Unit and slice of the calling CTA's item (blockIdx.x); false if the CTA has no item.
-__device__ __forceinline__ bool work_item(const WorkList& wl, u32& unit, u32& slice) {
-  const u32 i = blockIdx.x;
+// The WorkList that build_work_list returns for the same arguments, without launching anything.
+WorkList describe_work_list(const UnitMap& m, i64 M, const WorkScratch& s);
+// Unit and slice of item i; false if i is past the list's items.
+__device__ __forceinline__ bool work_item_at(const WorkList& wl, u32 i, u32& unit, u32& slice) {
   if (i >= wl.start[wl.units]) return false;
   unit = wl.owner[i];
   slice = i - wl.start[unit];
   return true;
+}
+// Unit and slice of the calling CTA's item (blockIdx.x); false if the CTA has no item.
+__device__ __forceinline__ bool work_item(const WorkList& wl, u32& unit, u32& slice) {
+  return work_item_at(wl, blockIdx.x, unit, slice);
 }
 // Points [begin, end) of slice `slice` of a bin's range [b0, b1).
 __device__ __forceinline__ void work_slice(u32 b0, u32 b1, u32 slice, u32 cap, u32& begin,
@@ -101,6 +106,44 @@ template <typename T>
 void launch_interp(const InterpArgs<T>& a, cudaStream_t stream);
 template <typename T>
 void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream);
+
+// ---- z-window kernels over many transforms (zwin.cu) --------------------------------------------
+// Plane chunks of the z-window kernels: each (x, y) column is cut into `count` chunks of `len`
+// planes, one launch unit each.
+struct ZChunks {
+  int len;    // planes per chunk
+  int count;  // chunks per column
+};
+// One transform's share of a persistent launch: its arguments, chunks and work list.
+template <typename T>
+struct ZSpreadJob {
+  SpreadArgs<T> a;
+  ZChunks ch;
+  WorkList wl;
+};
+template <typename T>
+struct ZInterpJob {
+  InterpArgs<T> a;
+  ZChunks ch;
+  WorkList wl;
+};
+// Host-side descriptions (nothing is launched); the work lists they name are built on the
+// device by zwin_build_work_list, which must run before the persistent launch.
+template <typename T>
+ZSpreadJob<T> zwin_spread_job(const SpreadArgs<T>& a);
+template <typename T>
+ZInterpJob<T> zwin_interp_job(const InterpArgs<T>& a);
+template <typename T>
+void zwin_build_work_list(const BinGeom& g, const SortedPoints<T>& pts, cudaStream_t stream);
+// One persistent launch over the items of njobs transforms that share (T, w, tile x): CTAs take
+// items from the counter *queue (zero at launch) until all `total` items are taken; item_end
+// holds the jobs' cumulative item counts. Jobs, item_end and queue are device memory.
+template <typename T>
+void launch_spread_zwin_fused(const ZSpreadJob<T>* jobs, const i64* item_end, int njobs,
+                              i64 total, int w, int tile_x, u32* queue, cudaStream_t stream);
+template <typename T>
+void launch_interp_zwin_fused(const ZInterpJob<T>* jobs, const i64* item_end, int njobs,
+                              i64 total, int w, int tile_x, u32* queue, cudaStream_t stream);
 
 // ---- deconvolution (deconv.cu) --------------------------------------------------------------
 template <typename T>

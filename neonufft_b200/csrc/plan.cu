@@ -45,6 +45,16 @@ void check_strides(int dim, const i64* modes, const i64* strides) {
 
 }  // namespace
 
+void PlanBase::fused_job(int, const void*, void*, void*) const {
+  throw_internal("plan has no persistent z-window step");
+}
+void PlanBase::fused_pre(int, const void*, const i64*) {
+  throw_internal("plan has no persistent z-window step");
+}
+void PlanBase::fused_post(int, void*, const i64*) {
+  throw_internal("plan has no persistent z-window step");
+}
+
 void validate_options(const NnbOptions& opt) {
   if (!(opt.tol > 0.0) || !std::isfinite(opt.tol)) throw_input("tol must be positive and finite");
   if (!(opt.upsampfac > 1.0) || !std::isfinite(opt.upsampfac)) {
@@ -116,21 +126,7 @@ public:
     NNB_CUDA(cudaMemsetAsync(fft_->data(), 0, sizeof(cplx_t<T>) * fft_->cells(), stream_));
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_SPREAD);
-      if (M > 0) {
-        SpreadArgs<T> a{};
-        a.g = geom_;
-        a.pts = points_.view();
-        a.in = static_cast<const cplx_t<T>*>(in);
-        a.prephase = nullptr;
-        a.grid = fft_->data();
-        a.in_bdist = 0;
-        a.grid_bdist = 0;
-        a.batch = 1;
-        a.beta = T(kp_.beta);
-        a.c = T(kp_.c);
-        a.method = method_;
-        launch_spread<T>(a, stream_);
-      }
+      if (M > 0) launch_spread<T>(spread_args(in), stream_);
     }
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
@@ -159,17 +155,44 @@ public:
     }
     if (M > 0) {
       ScopedStage st(timer_, stream_, NNB_STAGE_INTERP);
-      InterpArgs<T> a{};
-      a.g = geom_;
-      a.pts = points_.view();
-      a.grid = fft_->data();
-      a.postphase = nullptr;
-      a.out = static_cast<cplx_t<T>*>(out);
-      a.beta = T(kp_.beta);
-      a.c = T(kp_.c);
-      a.method = method_;
-      launch_interp<T>(a, stream_);
+      launch_interp<T>(interp_args(out), stream_);
     }
+  }
+
+  bool fused_key(int* key) const override {
+    if (method_ != 3 || dim_ != 3 || points_.size() == 0) return false;
+    *key = kp_.w | (tile_[0] << 8);
+    return true;
+  }
+
+  void fused_job(int type, const void* in, void* out, void* job) const override {
+    int key;
+    if (!fused_key(&key)) throw_internal("plan has no persistent z-window step");
+    if (type == 1) {
+      *static_cast<ZSpreadJob<T>*>(job) = zwin_spread_job<T>(spread_args(in));
+    } else {
+      *static_cast<ZInterpJob<T>*>(job) = zwin_interp_job<T>(interp_args(out));
+    }
+  }
+
+  void fused_pre(int type, const void* in, const i64* strides) override {
+    check_strides(dim_, modes_, strides);
+    if (type == 1) {
+      NNB_CUDA(cudaMemsetAsync(fft_->data(), 0, sizeof(cplx_t<T>) * fft_->cells(), stream_));
+    } else {
+      launch_upsample<T>(deconv_args(strides), static_cast<const cplx_t<T>*>(in), fft_->data(),
+                         stream_);
+      fft_->exec(stream_);
+    }
+    zwin_build_work_list<T>(geom_, points_.view(), stream_);
+  }
+
+  void fused_post(int type, void* out, const i64* strides) override {
+    if (type != 1) return;
+    check_strides(dim_, modes_, strides);
+    fft_->exec(stream_);
+    launch_downsample<T>(deconv_args(strides), fft_->data(), static_cast<cplx_t<T>*>(out),
+                         stream_);
   }
 
   void info(NnbPlanInfo* info) const override {
@@ -194,6 +217,35 @@ public:
   cudaStream_t stream() const override { return stream_; }
 
 private:
+  SpreadArgs<T> spread_args(const void* in) const {
+    SpreadArgs<T> a{};
+    a.g = geom_;
+    a.pts = points_.view();
+    a.in = static_cast<const cplx_t<T>*>(in);
+    a.prephase = nullptr;
+    a.grid = fft_->data();
+    a.in_bdist = 0;
+    a.grid_bdist = 0;
+    a.batch = 1;
+    a.beta = T(kp_.beta);
+    a.c = T(kp_.c);
+    a.method = method_;
+    return a;
+  }
+
+  InterpArgs<T> interp_args(void* out) const {
+    InterpArgs<T> a{};
+    a.g = geom_;
+    a.pts = points_.view();
+    a.grid = fft_->data();
+    a.postphase = nullptr;
+    a.out = static_cast<cplx_t<T>*>(out);
+    a.beta = T(kp_.beta);
+    a.c = T(kp_.c);
+    a.method = method_;
+    return a;
+  }
+
   DeconvArgs<T> deconv_args(const i64* strides) const {
     DeconvArgs<T> a{};
     a.dim = dim_;

@@ -21,6 +21,22 @@ public:
   virtual void info(NnbPlanInfo* info) const = 0;
   virtual StageTimer& timer() = 0;
   virtual cudaStream_t stream() const = 0;
+
+  // Hooks for persistent batched execution (batch.cu): a plan whose spreading or interpolation
+  // runs on the z-window kernels can leave that step of a transform to one persistent launch
+  // over many plans. fused_key is false if the plan cannot, else a key that is equal for plans
+  // one launch can serve (precision aside: a batch has one).
+  virtual bool fused_key(int* key) const {
+    (void)key;
+    return false;
+  }
+  // Host description of the step of transform `type` (a ZSpreadJob<T> or ZInterpJob<T>).
+  virtual void fused_job(int type, const void* in, void* out, void* job) const;
+  // Work before the step, on the plan's stream: type 1 clears the fine grid; type 2 deconvolves
+  // `in` into it and transforms it; both build the step's work list.
+  virtual void fused_pre(int type, const void* in, const i64* strides);
+  // Work after the step, on the plan's stream: type 1 transforms and deconvolves into `out`.
+  virtual void fused_post(int type, void* out, const i64* strides);
 };
 
 class PlanT3Base {

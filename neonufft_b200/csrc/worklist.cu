@@ -52,22 +52,27 @@ __global__ void __launch_bounds__(kWlThreads)
 
 }  // namespace
 
-WorkList build_work_list(const UnitMap& m, const BinGeom& g, const u32* bin_start, i64 M,
-                         const WorkScratch& s, cudaStream_t stream) {
+WorkList describe_work_list(const UnitMap& m, i64 M, const WorkScratch& s) {
   if (m.units < 1 || m.units > s.max_units) throw_internal("work list larger than its scratch");
   WorkList wl;
   wl.units = m.units;
   wl.cap = kWorkItemPoints;
   wl.grid = m.units + (M + kWorkItemPoints - 1) / kWorkItemPoints + 1;
   if (wl.grid > s.max_items) throw_internal("work list larger than its scratch");
+  wl.owner = s.owner;
+  wl.start = s.start;
+  return wl;
+}
+
+WorkList build_work_list(const UnitMap& m, const BinGeom& g, const u32* bin_start, i64 M,
+                         const WorkScratch& s, cudaStream_t stream) {
+  const WorkList wl = describe_work_list(m, M, s);
   const unsigned blocks = unsigned((m.units + kWlThreads - 1) / kWlThreads);
   unit_items_kernel<<<blocks, kWlThreads, 0, stream>>>(m, g, bin_start, wl.cap, s.cnt);
   NNB_LAUNCH_CHECK();
   launch_exclusive_scan(s.cnt, s.start, m.units, s.tmp, stream);
   owner_kernel<<<blocks, kWlThreads, 0, stream>>>(m.units, s.start, s.owner);
   NNB_LAUNCH_CHECK();
-  wl.owner = s.owner;
-  wl.start = s.start;
   return wl;
 }
 

@@ -123,6 +123,13 @@ struct ZShape {
   static constexpr int P1 = TY + W - 1;             // region y extent
   static constexpr int BATCH = sizeof(T) == 4 ? 64 : 32;  // points staged at a time
   static constexpr int G = 8;                       // points reduced together (interpolation)
+  // CTAs per SM the interpolation kernel is compiled for: uncapped, it took 96 registers and
+  // spilled; capped at 5, 87 (float) / 96 (double) registers without spills, 3 % faster.
+  static constexpr int INTERP_CTAS = 5;
+  // CTAs per SM the persistent kernels are compiled for: without the cap, their loop over items
+  // lets the register allocator grow far past the per-transform kernels (166 against 72).
+  static constexpr int SPREAD_FUSED_CTAS = sizeof(T) == 4 ? 7 : 4;
+  static constexpr int INTERP_FUSED_CTAS = sizeof(T) == 4 ? 6 : 4;
   static_assert(W <= RZ && P1 <= RY, "window smaller than the kernel footprint");
   static_assert(BATCH % NWARP == 0 && BATCH / NWARP <= 32, "staging threads");
 };
@@ -214,12 +221,6 @@ __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX>* slots, const PointRe
   }
 }
 
-// Chunk of planes handled by one CTA.
-struct ZChunks {
-  int len;    // planes per chunk
-  int count;  // chunks per column
-};
-
 // base + off wrapped to [0, n) for 0 <= base < n, 0 <= off.
 __device__ __forceinline__ i64 wrap_add(i64 base, int off, i64 n) {
   i64 i = base + off;
@@ -262,9 +263,9 @@ struct ZCta {
   u32 pbeg, pend;
 };
 __device__ __forceinline__ bool zcta(const BinGeom& g, const u32* bin_start, ZChunks ch,
-                                     const WorkList& wl, ZCta& c) {
+                                     const WorkList& wl, u32 item, ZCta& c) {
   u32 unit, slice;
-  if (!work_item(wl, unit, slice)) return false;
+  if (!work_item_at(wl, item, unit, slice)) return false;
   const i64 ncols = i64(g.ntiles[0]) * g.ntiles[1];
   const int chunk = int(unit / ncols);
   const i64 col = unit - i64(chunk) * ncols;
@@ -301,20 +302,26 @@ struct ZThread {
 
 // ---- spreading ---------------------------------------------------------------------------------
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
-    spread_zwin_kernel(SpreadArgs<T> a, ZChunks ch, WorkList wl) {
+struct ZSpreadShared {
+  ZSlot<T, W, TX> slots[2][ZShape<T, W, TX>::BATCH];
+};
+
+// Spreads work item `item` of batch entry `batch` (one CTA; every thread calls it).
+template <typename T, int W, int TX>
+__device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks ch,
+                                                 const WorkList& wl, u32 item, int batch,
+                                                 ZSpreadShared<T, W, TX>& sh) {
   using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
   using Slot = ZSlot<T, W, TX>;
-  __shared__ Slot slots[2][S::BATCH];
+  auto& slots = sh.slots;
 
   const BinGeom& g = a.g;
   ZCta cta;
-  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
+  if (!zcta(g, a.pts.bin_start, ch, wl, item, cta)) return;
   const ZThread<T, W, TX> th;
-  const int batch = blockIdx.y;
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
@@ -426,6 +433,61 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   flush(cur + ((th.rb - cur) & (S::RZ - 1)));  // the rest of the window
 }
 
+template <typename T, int W, int TX>
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
+    spread_zwin_kernel(const __grid_constant__ SpreadArgs<T> a, ZChunks ch,
+                       const __grid_constant__ WorkList wl) {
+  __shared__ ZSpreadShared<T, W, TX> sh;
+  spread_zwin_item<T, W, TX>(a, ch, wl, blockIdx.x, int(blockIdx.y), sh);
+}
+
+// Takes the next item of the queue spanning all jobs; every thread returns the same values.
+// The job's record is copied to shared memory once per item.
+template <typename Job>
+__device__ __forceinline__ bool next_fused_item(const Job* jobs, const i64* item_end, int njobs,
+                                                i64 total, u32* queue, Job& job, u32& local) {
+  __shared__ i64 s_item;
+  __shared__ int s_job;
+  if (threadIdx.x == 0) {
+    const i64 it = i64(atomicAdd(queue, 1u));
+    int lo = 0, hi = njobs;  // first job whose cumulative item count exceeds it
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (item_end[mid] > it) {
+        hi = mid;
+      } else {
+        lo = mid + 1;
+      }
+    }
+    s_item = it;
+    s_job = lo;
+  }
+  __syncthreads();
+  const i64 it = s_item;
+  const int j = s_job;
+  if (it >= total || j >= njobs) return false;
+  static_assert(sizeof(Job) % 4 == 0, "job records are copied in words");
+  const int* src = reinterpret_cast<const int*>(jobs + j);
+  int* dst = reinterpret_cast<int*>(&job);
+  for (int k = int(threadIdx.x); k < int(sizeof(Job) / 4); k += int(blockDim.x)) dst[k] = src[k];
+  local = u32(it - (j > 0 ? item_end[j - 1] : 0));
+  __syncthreads();
+  return true;
+}
+
+template <typename T, int W, int TX>
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::SPREAD_FUSED_CTAS)
+    spread_zwin_fused_kernel(const ZSpreadJob<T>* jobs, const i64* item_end, int njobs,
+                             i64 total, u32* queue) {
+  __shared__ ZSpreadShared<T, W, TX> sh;
+  __shared__ ZSpreadJob<T> job;
+  u32 local;
+  while (next_fused_item(jobs, item_end, njobs, total, queue, job, local)) {
+    spread_zwin_item<T, W, TX>(job.a, job.ch, job.wl, local, 0, sh);
+    __syncthreads();  // the job record and the slots are rewritten for the next item
+  }
+}
+
 // ---- spreading on the tensor cores (method 4, single precision, 5 <= w <= 8) ---------------------
 //
 // The same window, staging and flushes as spread_zwin_kernel, with the per-point row updates
@@ -483,7 +545,7 @@ __global__ void __launch_bounds__(128) spread_zmma_kernel(SpreadArgs<float> a, Z
 
   const BinGeom& g = a.g;
   ZCta cta;
-  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
+  if (!zcta(g, a.pts.bin_start, ch, wl, blockIdx.x, cta)) return;
   const ZThread<float, W, TX> th;
   const int gq = th.lane >> 2;  // fragment row group
   const int tq = th.lane & 3;   // thread in group
@@ -618,23 +680,34 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
-    interp_zwin_kernel(InterpArgs<T> a, ZChunks ch, WorkList wl) {
+struct ZInterpShared {
+  using S = ZShape<T, W, TX>;
+  static constexpr int RS = 33;  // odd row stride of the transpose buffer: conflict-free reads
+  ZSlot<T, W, TX> slots[2][S::BATCH];
+  cplx_t<T> red[S::NWARP][S::G][RS];
+  cplx_t<T> res[2][S::NWARP][S::BATCH];
+  cplx_t<T> stage_row[S::RY][2 * S::NP];  // next plane of the loading threads' rows
+};
+
+// Interpolates work item `item` (one CTA; every thread calls it).
+template <typename T, int W, int TX>
+__device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks ch,
+                                                 const WorkList& wl, u32 item,
+                                                 ZInterpShared<T, W, TX>& sh) {
   using S = ZShape<T, W, TX>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
   using Slot = ZSlot<T, W, TX>;
   constexpr int G = S::G;
-  constexpr int RS = 33;  // odd row stride of the transpose buffer: conflict-free reads
-  __shared__ Slot slots[2][S::BATCH];
-  __shared__ C red[S::NWARP][G][RS];
-  __shared__ C res[2][S::NWARP][S::BATCH];
-  __shared__ C stage_row[S::RY][2 * S::NP];  // next plane of the loading threads' rows
+  auto& slots = sh.slots;
+  auto& red = sh.red;
+  auto& res = sh.res;
+  auto& stage_row = sh.stage_row;
 
   const BinGeom& g = a.g;
   ZCta cta;
-  if (!zcta(g, a.pts.bin_start, ch, wl, cta)) return;
+  if (!zcta(g, a.pts.bin_start, ch, wl, item, cta)) return;
   const ZThread<T, W, TX> th;
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
@@ -839,6 +912,27 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
   if (pending) cp_async_wait_all();
 }
 
+template <typename T, int W, int TX>
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::INTERP_CTAS)
+    interp_zwin_kernel(const __grid_constant__ InterpArgs<T> a, ZChunks ch,
+                       const __grid_constant__ WorkList wl) {
+  __shared__ ZInterpShared<T, W, TX> sh;
+  interp_zwin_item<T, W, TX>(a, ch, wl, blockIdx.x, sh);
+}
+
+template <typename T, int W, int TX>
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::INTERP_FUSED_CTAS)
+    interp_zwin_fused_kernel(const ZInterpJob<T>* jobs, const i64* item_end, int njobs,
+                             i64 total, u32* queue) {
+  __shared__ ZInterpShared<T, W, TX> sh;
+  __shared__ ZInterpJob<T> job;
+  u32 local;
+  while (next_fused_item(jobs, item_end, njobs, total, queue, job, local)) {
+    interp_zwin_item<T, W, TX>(job.a, job.ch, job.wl, local, sh);
+    __syncthreads();  // the job record and the shared buffers are rewritten for the next item
+  }
+}
+
 ZChunks make_chunks(i64 ncols, int nz, int w) {
   // About four waves of 8 CTAs per SM; chunks of at least 4 w planes bound the window
   // overhead (w - 1 extra planes flushed, or RZ planes loaded, per chunk).
@@ -854,17 +948,27 @@ ZChunks make_chunks(i64 ncols, int nz, int w) {
   return ch;
 }
 
-// Work list of (column, chunk) units split into items of at most kWorkItemPoints points.
-template <typename T>
-WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch,
-                        cudaStream_t stream) {
+// Launch units of a plane-major point set: (column, chunk) pairs.
+UnitMap zwin_unit_map(const BinGeom& g, ZChunks ch) {
   UnitMap m{};
   m.kind = UnitMap::kZwin;
   m.ncols = i64(g.ntiles[0]) * g.ntiles[1];
   m.units = m.ncols * ch.count;
   m.nz = g.ntiles[2];
   m.zlen = ch.len;
-  const WorkList wl = build_work_list(m, g, pts.bin_start, pts.M, pts.work, stream);
+  return m;
+}
+
+ZChunks zwin_chunks(const BinGeom& g) {
+  return make_chunks(i64(g.ntiles[0]) * g.ntiles[1], g.ntiles[2], g.w);
+}
+
+// Work list of (column, chunk) units split into items of at most kWorkItemPoints points.
+template <typename T>
+WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch,
+                        cudaStream_t stream) {
+  const WorkList wl = build_work_list(zwin_unit_map(g, ch), g, pts.bin_start, pts.M, pts.work,
+                                      stream);
   if (wl.grid > 0x7fffffffll) throw_input("grid too large");
   return wl;
 }
@@ -925,6 +1029,60 @@ void check_zwin_geom(const BinGeom& g) {
   }
 }
 
+
+// Persistent launches: as many CTAs as fit on the GPU at once, or fewer when there are fewer
+// items; each takes items from the shared queue until it is empty.
+template <typename K>
+unsigned persistent_grid(K kernel, int threads, i64 total) {
+  int dev = 0, sms = 0, per_sm = 0;
+  NNB_CUDA(cudaGetDevice(&dev));
+  NNB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  NNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+  i64 g = i64(sms) * (per_sm > 0 ? per_sm : 1);
+  if (g > total) g = total;
+  return unsigned(g < 1 ? 1 : g);
+}
+
+template <typename T, int W, int TX>
+void spread_fused_tw(const ZSpreadJob<T>* jobs, const i64* item_end, int njobs, i64 total,
+                     u32* queue, cudaStream_t stream) {
+  constexpr int NT = ZShape<T, W, TX>::NT;
+  const unsigned grid = persistent_grid(spread_zwin_fused_kernel<T, W, TX>, NT, total);
+  spread_zwin_fused_kernel<T, W, TX><<<grid, NT, 0, stream>>>(jobs, item_end, njobs, total,
+                                                              queue);
+  NNB_LAUNCH_CHECK();
+}
+
+template <typename T, int W, int TX>
+void interp_fused_tw(const ZInterpJob<T>* jobs, const i64* item_end, int njobs, i64 total,
+                     u32* queue, cudaStream_t stream) {
+  constexpr int NT = ZShape<T, W, TX>::NT;
+  const unsigned grid = persistent_grid(interp_zwin_fused_kernel<T, W, TX>, NT, total);
+  interp_zwin_fused_kernel<T, W, TX><<<grid, NT, 0, stream>>>(jobs, item_end, njobs, total,
+                                                              queue);
+  NNB_LAUNCH_CHECK();
+}
+
+// Calls f(std::integral_constant<int, w>) for 2 <= w <= 8.
+template <typename F>
+void with_width(int w, F&& f) {
+  switch (w) {
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    default: throw_internal("z-window kernels need n_spread <= 8");
+  }
+}
+
+void check_fused(int njobs, i64 total, int tile_x) {
+  if (njobs < 1) throw_internal("a persistent launch needs at least one job");
+  if (total < 1 || total > 0x7fffffffll) throw_internal("persistent launch item count out of range");
+  if (tile_x != 4 && tile_x != 8) throw_internal("z-window kernels need tiles of 4 or 8 in x");
+}
 }  // namespace
 
 template <int W>
@@ -965,6 +1123,78 @@ void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream) {
   return interp_zwin_tx<T, 4>(a, stream);
 }
 
+template <typename T>
+ZSpreadJob<T> zwin_spread_job(const SpreadArgs<T>& a) {
+  check_zwin_geom(a.g);
+  if (a.method != 3 || a.batch != 1) throw_internal("persistent spreading is method 3, batch 1");
+  ZSpreadJob<T> j;
+  j.a = a;
+  j.ch = zwin_chunks(a.g);
+  j.wl = describe_work_list(zwin_unit_map(a.g, j.ch), a.pts.M, a.pts.work);
+  return j;
+}
+
+template <typename T>
+ZInterpJob<T> zwin_interp_job(const InterpArgs<T>& a) {
+  check_zwin_geom(a.g);
+  if (a.method != 3) throw_internal("persistent interpolation is method 3");
+  ZInterpJob<T> j;
+  j.a = a;
+  j.ch = zwin_chunks(a.g);
+  j.wl = describe_work_list(zwin_unit_map(a.g, j.ch), a.pts.M, a.pts.work);
+  return j;
+}
+
+template <typename T>
+void zwin_build_work_list(const BinGeom& g, const SortedPoints<T>& pts, cudaStream_t stream) {
+  check_zwin_geom(g);
+  (void)zwin_work_list(g, pts, zwin_chunks(g), stream);
+}
+
+template <typename T>
+void launch_spread_zwin_fused(const ZSpreadJob<T>* jobs, const i64* item_end, int njobs,
+                              i64 total, int w, int tile_x, u32* queue, cudaStream_t stream) {
+  check_fused(njobs, total, tile_x);
+  with_width(w, [&](auto wc) {
+    constexpr int W = decltype(wc)::value;
+    if (tile_x == 8) {
+      spread_fused_tw<T, W, 8>(jobs, item_end, njobs, total, queue, stream);
+    } else {
+      spread_fused_tw<T, W, 4>(jobs, item_end, njobs, total, queue, stream);
+    }
+  });
+}
+
+template <typename T>
+void launch_interp_zwin_fused(const ZInterpJob<T>* jobs, const i64* item_end, int njobs,
+                              i64 total, int w, int tile_x, u32* queue, cudaStream_t stream) {
+  check_fused(njobs, total, tile_x);
+  with_width(w, [&](auto wc) {
+    constexpr int W = decltype(wc)::value;
+    if (tile_x == 8) {
+      interp_fused_tw<T, W, 8>(jobs, item_end, njobs, total, queue, stream);
+    } else {
+      interp_fused_tw<T, W, 4>(jobs, item_end, njobs, total, queue, stream);
+    }
+  });
+}
+
+template ZSpreadJob<float> zwin_spread_job<float>(const SpreadArgs<float>&);
+template ZSpreadJob<double> zwin_spread_job<double>(const SpreadArgs<double>&);
+template ZInterpJob<float> zwin_interp_job<float>(const InterpArgs<float>&);
+template ZInterpJob<double> zwin_interp_job<double>(const InterpArgs<double>&);
+template void zwin_build_work_list<float>(const BinGeom&, const SortedPoints<float>&,
+                                          cudaStream_t);
+template void zwin_build_work_list<double>(const BinGeom&, const SortedPoints<double>&,
+                                           cudaStream_t);
+template void launch_spread_zwin_fused<float>(const ZSpreadJob<float>*, const i64*, int, i64,
+                                              int, int, u32*, cudaStream_t);
+template void launch_spread_zwin_fused<double>(const ZSpreadJob<double>*, const i64*, int, i64,
+                                               int, int, u32*, cudaStream_t);
+template void launch_interp_zwin_fused<float>(const ZInterpJob<float>*, const i64*, int, i64,
+                                              int, int, u32*, cudaStream_t);
+template void launch_interp_zwin_fused<double>(const ZInterpJob<double>*, const i64*, int, i64,
+                                               int, int, u32*, cudaStream_t);
 template void launch_spread_zwin<float>(const SpreadArgs<float>&, cudaStream_t);
 template void launch_spread_zwin<double>(const SpreadArgs<double>&, cudaStream_t);
 template void launch_interp_zwin<float>(const InterpArgs<float>&, cudaStream_t);

@@ -329,9 +329,12 @@ def _info_dict(i: L.NnbPlanInfo) -> dict:
 class Batch:
     """Many independent type-1 / type-2 transforms of uneven sizes run together (engine
     extension, nnb_batch_* in include/neonufft_gpu.h): one plan per transform on internal streams,
-    executed serially, concurrently, or as one captured CUDA graph."""
+    executed serially, concurrently, or as one captured CUDA graph; the FUSED modes also run the
+    z-window spreading / interpolation steps of all 3D transforms as persistent launches over one
+    queue of their work items."""
 
     SERIAL, STREAMS, GRAPH = L.NNB_BATCH_SERIAL, L.NNB_BATCH_STREAMS, L.NNB_BATCH_GRAPH
+    FUSED, FUSED_GRAPH = L.NNB_BATCH_FUSED, L.NNB_BATCH_FUSED_GRAPH
 
     def __init__(self, opt: Options, dtype, num_streams: int = 4, stream=None,
                  device_alloc=None):
