@@ -39,26 +39,64 @@ __device__ __forceinline__ bool cell_of(const BinGeom& g, int d, double x, i64& 
   return true;
 }
 
+// Points per thread and loop trip: the kernels are bound by memory latency (the coordinate
+// loads, the rank atomic, the bin-offset gather), so each thread keeps kBinUnroll independent
+// points in flight; point u of a trip is base + u * stride, so every load stays coalesced.
+constexpr int kBinUnroll = 4;
+
+// tile_linear with the dimension known at compile time (registers instead of a local array).
+template <int DIM>
+__device__ __forceinline__ i64 tile_linear_d(const BinGeom& g, const i64 (&t)[3]) {
+  if (DIM == 3 && g.zmajor) return t[2] + i64(g.ntiles[2]) * (t[0] + i64(g.ntiles[0]) * t[1]);
+  i64 lin = 0, mul = 1;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    lin += t[d] * mul;
+    mul *= g.ntiles[d];
+  }
+  return lin;
+}
+
 template <typename T, int DIM>
 __global__ void __launch_bounds__(kBinBlock)
     bin_count_kernel(BinGeom g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks, int* err) {
-  for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
-       i += i64(gridDim.x) * kBinBlock) {
-    i64 t[3] = {0, 0, 0};
-    bool ok = true;
+  const i64 stride = i64(gridDim.x) * kBinBlock;
+  for (i64 base = blockIdx.x * i64(kBinBlock) + threadIdx.x; base < M;
+       base += stride * kBinUnroll) {
+    T v[kBinUnroll][DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      i64 i0 = 0;
-      double frac;
-      ok &= cell_of(g, d, double(x.p[d][i]), i0, frac);
-      t[d] = i0 / g.tile[d];
+    for (int u = 0; u < kBinUnroll; ++u) {
+      const i64 i = base + u * stride;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[u][d] = i < M ? x.p[d][i] : T(0);
     }
-    i64 tile_lin = tile_linear(g, t);
-    if (!ok) {
-      atomicOr(err, 1);
-      tile_lin = 0;
+    i64 tile_lin[kBinUnroll];
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      i64 t[3] = {0, 0, 0};
+      bool ok = true;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        i64 i0 = 0;
+        double frac;
+        ok &= cell_of(g, d, double(v[u][d]), i0, frac);
+        t[d] = i0 / g.tile[d];
+      }
+      tile_lin[u] = tile_linear_d<DIM>(g, t);
+      if (!ok && base + u * stride < M) {
+        atomicOr(err, 1);
+        tile_lin[u] = 0;
+      }
     }
-    ranks[i] = atomicAdd(&counts[tile_lin], 1u);
+    u32 r[kBinUnroll];
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      if (base + u * stride < M) r[u] = atomicAdd(&counts[tile_lin[u]], 1u);
+    }
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      if (base + u * stride < M) ranks[base + u * stride] = r[u];
+    }
   }
 }
 
@@ -66,36 +104,57 @@ template <typename T, int DIM>
 __global__ void __launch_bounds__(kBinBlock)
     bin_scatter_kernel(BinGeom g, CoordPtrs<T> x, i64 M, const u32* ranks, const u32* bin_start,
                        PointRec<T>* recs) {
-  for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
-       i += i64(gridDim.x) * kBinBlock) {
-    i64 t[3] = {0, 0, 0};
-    int l[3] = {0, 0, 0};
-    double fr[3] = {0, 0, 0};
-    i64 i0[3] = {0, 0, 0};
-    bool ok = true;
+  const i64 stride = i64(gridDim.x) * kBinBlock;
+  for (i64 base = blockIdx.x * i64(kBinBlock) + threadIdx.x; base < M;
+       base += stride * kBinUnroll) {
+    T v[kBinUnroll][DIM];
+    u32 rank[kBinUnroll];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) ok &= cell_of(g, d, double(x.p[d][i]), i0[d], fr[d]);
-    // A non-finite point went to tile 0 in pass 1 (the host then rejects the point set); it
-    // must land in the same tile here so that its slot stays inside tile 0's range.
+    for (int u = 0; u < kBinUnroll; ++u) {
+      const i64 i = base + u * stride;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      if (!ok) {
-        i0[d] = 0;
-        fr[d] = -0.5 * g.w;
-      }
-      t[d] = i0[d] / g.tile[d];
-      l[d] = int(i0[d] - t[d] * g.tile[d]);
+      for (int d = 0; d < DIM; ++d) v[u][d] = i < M ? x.p[d][i] : T(0);
+      rank[u] = i < M ? ranks[i] : 0u;
     }
-    const i64 tile_lin = tile_linear(g, t);
-    const u32 pos = bin_start[tile_lin] + ranks[i];
-    PointRec<T> r;
-    r.perm = u32(i);
-    r.local = (DIM == 3 && g.zmajor) ? pack_local_zmajor(l[0], l[1], i0[2])
-                                     : pack_local(DIM, l[0], l[1], l[2]);
-    r.frac[0] = T(fr[0]);
-    r.frac[1] = T(fr[1]);
-    r.frac[2] = T(fr[2]);
-    recs[pos] = r;
+    PointRec<T> r[kBinUnroll];
+    i64 tile_lin[kBinUnroll];
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      i64 t[3] = {0, 0, 0};
+      int l[3] = {0, 0, 0};
+      double fr[3] = {0, 0, 0};
+      i64 i0[3] = {0, 0, 0};
+      bool ok = true;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) ok &= cell_of(g, d, double(v[u][d]), i0[d], fr[d]);
+      // A non-finite point went to tile 0 in pass 1 (the host then rejects the point set); it
+      // must land in the same tile here so that its slot stays inside tile 0's range.
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        if (!ok) {
+          i0[d] = 0;
+          fr[d] = -0.5 * g.w;
+        }
+        t[d] = i0[d] / g.tile[d];
+        l[d] = int(i0[d] - t[d] * g.tile[d]);
+      }
+      tile_lin[u] = tile_linear_d<DIM>(g, t);
+      r[u].perm = u32(base + u * stride);
+      r[u].local = (DIM == 3 && g.zmajor) ? pack_local_zmajor(l[0], l[1], i0[2])
+                                          : pack_local(DIM, l[0], l[1], l[2]);
+      r[u].frac[0] = T(fr[0]);
+      r[u].frac[1] = T(fr[1]);
+      r[u].frac[2] = T(fr[2]);
+    }
+    u32 pos[kBinUnroll];
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      if (base + u * stride < M) pos[u] = bin_start[tile_lin[u]] + rank[u];
+    }
+#pragma unroll
+    for (int u = 0; u < kBinUnroll; ++u) {
+      if (base + u * stride < M) recs[pos[u]] = r[u];
+    }
   }
 }
 
