@@ -61,8 +61,8 @@ WORKLOADS = {
 # of the same configuration (profiles/zwin_c2.md): (workload, precision, method, n_spread, tile,
 # kernel) -> bytes per point.
 DRAM_BYTES_PER_POINT = {
-    ("c2", "f32", 3, 8, (8, 8, 1), "interp"): (666.094080e6 + 262.095616e6) / 1e7,
-    ("c2", "f32", 3, 8, (8, 8, 1), "spread"): (944.648704e6 + 131.523328e6) / 1e7,
+    ("c2", "f32", 3, 8, (8, 8, 1), "interp"): (665.430528e6 + 261.607424e6) / 1e7,
+    ("c2", "f32", 3, 8, (8, 8, 1), "spread"): (943.662592e6 + 131.524864e6) / 1e7,
 }
 
 METRIC = "NU points/sec per transform at rel-l2 <=1e-6 (tuned FP32 vs plain GPU; CPU ref)"
