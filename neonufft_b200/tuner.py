@@ -62,7 +62,7 @@ def resolved(p: Problem, c: Config):
     """(kernel width, method, x tile) that a plan with configuration c uses."""
     w = c.n_spread or heuristic_width(p.tol, c.upsampfac, p.precision)
     method = c.method or (3 if p.dim == 3 and w <= 8 else 1)
-    tile0 = c.tile[0] or ((8 if p.precision == "f32" else 4) if method == 3 else 0)
+    tile0 = c.tile[0] or (4 if method == 3 else 0)
     return w, method, tile0
 
 
