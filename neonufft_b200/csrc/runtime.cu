@@ -278,8 +278,8 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
     // at M = 1e8, interpolation unchanged).
     tile[0] = 4;
     if (explicit_tile) {
-      if (requested[0] != 4 && requested[0] != 8) {
-        throw_input("spread method 3 supports tiles of 4 or 8 cells in x");
+      if (requested[0] != 2 && requested[0] != 4 && requested[0] != 8) {
+        throw_input("spread method 3 supports tiles of 2, 4 or 8 cells in x");
       }
       tile[0] = requested[0];
     }

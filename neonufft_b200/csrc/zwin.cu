@@ -1024,7 +1024,7 @@ void interp_zwin_tx(const InterpArgs<T>& a, cudaStream_t stream) {
 
 void check_zwin_geom(const BinGeom& g) {
   if (g.dim != 3 || !g.zmajor || g.tile[1] != 8 || g.tile[2] != 1 ||
-      (g.tile[0] != 4 && g.tile[0] != 8) || g.w > 8) {
+      (g.tile[0] != 2 && g.tile[0] != 4 && g.tile[0] != 8) || g.w > 8) {
     throw_internal("z-window kernels need a 3D plane-major (4|8, 8, 1) tiling and n_spread <= 8");
   }
 }
@@ -1081,7 +1081,9 @@ void with_width(int w, F&& f) {
 void check_fused(int njobs, i64 total, int tile_x) {
   if (njobs < 1) throw_internal("a persistent launch needs at least one job");
   if (total < 1 || total > 0x7fffffffll) throw_internal("persistent launch item count out of range");
-  if (tile_x != 4 && tile_x != 8) throw_internal("z-window kernels need tiles of 4 or 8 in x");
+  if (tile_x != 2 && tile_x != 4 && tile_x != 8) {
+    throw_internal("z-window kernels need tiles of 2, 4 or 8 in x");
+  }
 }
 }  // namespace
 
@@ -1113,6 +1115,7 @@ void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream) {
     throw_internal("tensor-core spreading is single precision");
   }
   if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8>(a, stream);
+  if (a.g.tile[0] == 2) return spread_zwin_tx<T, 2>(a, stream);
   return spread_zwin_tx<T, 4>(a, stream);
 }
 
@@ -1120,6 +1123,7 @@ template <typename T>
 void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream) {
   check_zwin_geom(a.g);
   if (a.g.tile[0] == 8) return interp_zwin_tx<T, 8>(a, stream);
+  if (a.g.tile[0] == 2) return interp_zwin_tx<T, 2>(a, stream);
   return interp_zwin_tx<T, 4>(a, stream);
 }
 
@@ -1159,6 +1163,8 @@ void launch_spread_zwin_fused(const ZSpreadJob<T>* jobs, const i64* item_end, in
     constexpr int W = decltype(wc)::value;
     if (tile_x == 8) {
       spread_fused_tw<T, W, 8>(jobs, item_end, njobs, total, queue, stream);
+    } else if (tile_x == 2) {
+      spread_fused_tw<T, W, 2>(jobs, item_end, njobs, total, queue, stream);
     } else {
       spread_fused_tw<T, W, 4>(jobs, item_end, njobs, total, queue, stream);
     }
@@ -1173,6 +1179,8 @@ void launch_interp_zwin_fused(const ZInterpJob<T>* jobs, const i64* item_end, in
     constexpr int W = decltype(wc)::value;
     if (tile_x == 8) {
       interp_fused_tw<T, W, 8>(jobs, item_end, njobs, total, queue, stream);
+    } else if (tile_x == 2) {
+      interp_fused_tw<T, W, 2>(jobs, item_end, njobs, total, queue, stream);
     } else {
       interp_fused_tw<T, W, 4>(jobs, item_end, njobs, total, queue, stream);
     }

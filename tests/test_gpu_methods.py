@@ -98,7 +98,8 @@ def test_clustered_points(dtype, type_, method, cuda, engine, oracle):
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("w", [2, 8])
 @pytest.mark.parametrize("type_", [1, 2])
-def test_zwin_tiny_grid(dtype, w, type_, cuda, engine, oracle):
+@pytest.mark.parametrize("tx", [2, 4, 8])
+def test_zwin_tiny_grid(dtype, w, type_, tx, cuda, engine, oracle):
     """Fine grids of 2w cells per dimension: the tile's halo region wraps around the grid."""
     rng = np.random.default_rng(3 * w + type_)
     modes = [3, 2, 4]
@@ -107,7 +108,7 @@ def test_zwin_tiny_grid(dtype, w, type_, cuda, engine, oracle):
     n_in = M if type_ == 1 else int(np.prod(modes))
     inp = rng.standard_normal(n_in) + 1j * rng.standard_normal(n_in)
     out3, _ = run_t12(engine, cuda, dtype, -1, pts, inp, modes, type_, n_spread=w,
-                      spread_method=3)
+                      spread_method=3, tile=(tx, 8, 1))
     out1, _ = run_t12(engine, cuda, dtype, -1, pts, inp, modes, type_, n_spread=w,
                       spread_method=1)
     ref = direct(oracle, type_, -1, pts, inp, modes, dtype)
@@ -116,7 +117,7 @@ def test_zwin_tiny_grid(dtype, w, type_, cuda, engine, oracle):
 
 
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
-@pytest.mark.parametrize("tx", [4, 8])
+@pytest.mark.parametrize("tx", [2, 4, 8])
 def test_zwin_tile_widths(dtype, tx, cuda, engine, oracle):
     rng = np.random.default_rng(tx)
     modes = [33, 20, 18]
