@@ -49,6 +49,11 @@ WORKLOADS = {
                     "[1e5,1e7], N per dim 64-256 (3D <= 128), tol {1e-3,1e-6} FP32 and 1e-9 FP64, "
                     "uniform or blobs; MLP trained on 40, picks scored on 20 against the heuristic",
                tuner=60, train=40, seed=5),
+    "c5full": dict(name="tuner sweep: 500 seeded problems, dim {2,3}, type {1,2}, M log-uniform "
+                        "[1e5,1e8], N per dim 64-512, tol {1e-3,1e-6} FP32 and 1e-9 FP64, uniform "
+                        "or blobs; MLP trained on 400, picks scored on 100 against the heuristic",
+                   tuner=500, train=400, seed=5, m_range=(5, 8), n2=(64, 128, 256, 512),
+                   n3=(64, 128, 256, 512)),
     "c3": dict(name="type 3, M=K=5e6, sources uniform in a box of half-width 50, targets in "
                     "half-width 200, tol 1e-5: 2D at the literal extents (the 3D grids need "
                     "~1.5e14 B), 3D at half-widths 9 and 36",
@@ -408,9 +413,11 @@ def run_tuner(args, wl):
     for i in range(wl["tuner"]):
         dim = int(rng.choice([2, 3]))
         f64 = i % 5 == 4
-        N = int(rng.choice([64, 96, 128] if dim == 3 else [64, 128, 256]))
+        N = int(rng.choice(wl.get("n3", (64, 96, 128)) if dim == 3
+                           else wl.get("n2", (64, 128, 256))))
+        lo, hi = wl.get("m_range", (5, 7))
         problems.append(T.Problem(dim=dim, type=int(rng.choice([1, 2])),
-                                  M=int(10 ** rng.uniform(5, 7)), N=N,
+                                  M=int(10 ** rng.uniform(lo, hi)), N=N,
                                   tol=1e-9 if f64 else float(rng.choice([1e-3, 1e-6])),
                                   precision="f64" if f64 else "f32", blob=bool(rng.random() < 0.5),
                                   seed=i))
@@ -438,7 +445,8 @@ def run_tuner(args, wl):
         else:
             heur_fail += 1
         # the exhaustive autotuner's best candidate meeting tol, for comparison
-        best = min((T.measure(p, c, data) for c in T.candidates(p)),
+        best = min((T.measure_or_none(p, c, data) or (float("inf"), float("inf"))
+                    for c in T.candidates(p)),
                    key=lambda r: r[0] if r[1] <= p.tol else float("inf"))
         if best[1] <= p.tol:
             best_ratio.append(best[0] / ms)

@@ -185,6 +185,18 @@ def measure(p: Problem, c: Config, data: ProblemData = None, reps: int = 3):
     return float(np.median(times)), err
 
 
+def measure_or_none(p: Problem, c: Config, data: ProblemData = None):
+    """measure(), or None when the configuration does not fit in device memory or is refused
+    (an InputError for a shape the methods do not support)."""
+    from .plan import InputError, MemoryAllocError
+    try:
+        return measure(p, c, data)
+    except (InputError, MemoryAllocError):
+        import torch
+        torch.cuda.empty_cache()
+        return None
+
+
 class Tuner:
     """Heuristic, autotuner and learned picker over the candidates of a problem."""
 
@@ -197,8 +209,9 @@ class Tuner:
         for p in problems:
             data = ProblemData(p)
             for c in candidates(p):
-                ms, err = measure(p, c, data)
-                self.rows.append((features(p, c), math.log10(ms), err, p, c))
+                r = measure_or_none(p, c, data)
+                if r is not None:
+                    self.rows.append((features(p, c), math.log10(r[0]), r[1], p, c))
         return self.rows
 
     def autotune(self, p: Problem):
@@ -226,7 +239,7 @@ class Tuner:
         pred = self.model.predict(np.stack([features(p, c) for c in cands]))
         data = data or ProblemData(p)
         for tried, i in enumerate(np.argsort(pred), start=1):
-            ms, err = measure(p, cands[int(i)], data)
-            if err <= p.tol:
-                return cands[int(i)], (ms, err), tried
+            r = measure_or_none(p, cands[int(i)], data)
+            if r is not None and r[1] <= p.tol:
+                return cands[int(i)], r, tried
         return HEURISTIC, measure(p, HEURISTIC, data), len(cands)
