@@ -29,25 +29,32 @@ template <typename T, int DIM>
 __device__ __forceinline__ void stage_region(const BinGeom& g, const TileLayout& L, int nrows,
                                              int ext1d, i64 o0, i64 o1, i64 o2,
                                              const cplx_t<T>* grid, cplx_t<T>* tile) {
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  if (DIM == 1) {
+  if constexpr (DIM == 1) {
+    (void)L;
+    (void)nrows;
+    (void)o1;
+    (void)o2;
     for (int cx = threadIdx.x; cx < ext1d; cx += blockDim.x) {
       tile[cx] = grid[wrap_index(o0 + cx, g.nf[0])];
     }
-    return;
-  }
-  for (int row = warp; row < nrows; row += nwarps) {
-    int cy = row, cz = 0;
-    if (DIM == 3) {
-      cz = row / L.P1;
-      cy = row - cz * L.P1;
+  } else {
+    (void)ext1d;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int row = warp; row < nrows; row += nwarps) {
+      int cy = row, cz = 0;
+      if (DIM == 3) {
+        cz = row / L.P1;
+        cy = row - cz * L.P1;
+      }
+      i64 rbase = wrap_index(o1 + cy, g.nf[1]) * g.nf[0];
+      if (DIM == 3) rbase += wrap_index(o2 + cz, g.nf[2]) * g.nf[0] * g.nf[1];
+      cplx_t<T>* dst = tile + cz * L.PS + cy * L.RS;
+      for (int cx = lane; cx < L.P0; cx += 32) {
+        dst[cx] = grid[rbase + wrap_index(o0 + cx, g.nf[0])];
+      }
     }
-    i64 rbase = wrap_index(o1 + cy, g.nf[1]) * g.nf[0];
-    if (DIM == 3) rbase += wrap_index(o2 + cz, g.nf[2]) * g.nf[0] * g.nf[1];
-    cplx_t<T>* dst = tile + cz * L.PS + cy * L.RS;
-    for (int cx = lane; cx < L.P0; cx += 32) dst[cx] = grid[rbase + wrap_index(o0 + cx, g.nf[0])];
   }
 }
 

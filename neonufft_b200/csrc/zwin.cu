@@ -51,13 +51,13 @@ struct Packed<float> {
   }
   static __device__ __forceinline__ P splat(float x) { return pack(x, x); }
   static __device__ __forceinline__ float lo(P v) {
-    float x, y;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+    float x;
+    asm("mov.b64 {%0, _}, %1;" : "=f"(x) : "l"(v));
     return x;
   }
   static __device__ __forceinline__ float hi(P v) {
-    float x, y;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+    float y;
+    asm("mov.b64 {_, %0}, %1;" : "=f"(y) : "l"(v));
     return y;
   }
   // a * b + c, elementwise
@@ -392,8 +392,27 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
   for (int k = 0; k < nbatch; ++k) {
     const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
     const Slot* sb = slots[k & 1];
-    auto apply = [&](const Slot& sl, int lyp) {
-      if (th.owns(lyp & 15)) {
+    // The points of this batch whose footprint covers rows of this warp, one bit per slot: the
+    // warp visits only those, with a window of its own (no other warp touches its rows).
+    u32 own[S::BATCH / 32];
+#pragma unroll
+    for (int h = 0; h < S::BATCH / 32; ++h) {
+      const int j = h * 32 + th.lane;
+      own[h] = __ballot_sync(0xffffffffu, j < nb && th.owns(sb[j < nb ? j : 0].lyp & 15));
+    }
+#pragma unroll
+    for (int h = 0; h < S::BATCH / 32; ++h) {
+      for (u32 m = own[h]; m != 0u; m &= m - 1u) {
+        const Slot& sl = sb[h * 32 + __ffs(int(m)) - 1];
+        const int tp = sl.lyp >> 4;
+        if (tp != cur) {  // advance the window: planes [cur, tp) are complete
+          const int n = min(tp - cur, S::RZ);
+          for (int i = 0; i < n; ++i) {
+            if (th.rb == ((cur + i) & (S::RZ - 1))) flush(cur + i);
+          }
+          cur = tp;
+          dz = (th.rb - cur) & (S::RZ - 1);
+        }
         dirty = true;
         const T kw = sl.ky[th.ra] * sl.kz[dz];
         const C v = sl.v;
@@ -412,20 +431,6 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
           }
         }
       }
-    };
-    for (int j = 0; j < nb; ++j) {
-      const Slot& sl = sb[j];
-      const int lyp = sl.lyp;
-      const int tp = lyp >> 4;
-      if (tp != cur) {  // advance the window: planes [cur, tp) are complete
-        const int n = min(tp - cur, S::RZ);
-        for (int i = 0; i < n; ++i) {
-          if (th.rb == ((cur + i) & (S::RZ - 1))) flush(cur + i);
-        }
-        cur = tp;
-        dz = (th.rb - cur) & (S::RZ - 1);
-      }
-      apply(sl, lyp);
     }
     if (k + 1 < nbatch) stage(k + 1);
     __syncthreads();
