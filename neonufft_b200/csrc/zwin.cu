@@ -825,8 +825,16 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
   for (int k = 0; k < nbatch; ++k) {
     const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
     const Slot* sb = slots[k & 1];
-    auto partial = [&](const Slot& sl, int lyp) -> C {
-      if (!th.owns(lyp & 15)) return C{T(0), T(0)};
+    // The points of this batch whose footprint covers rows of this warp (bit j: slot j).
+    unsigned long long own = 0ull;
+#pragma unroll
+    for (int h = 0; h < (S::BATCH + 31) / 32; ++h) {
+      const int j = h * 32 + th.lane;
+      const u32 bits = __ballot_sync(0xffffffffu, j < nb && th.owns(sb[j < nb ? j : 0].lyp & 15));
+      own |= (unsigned long long)bits << (32 * h);
+    }
+    auto partial = [&](const Slot& sl, int j) -> C {
+      if (!((own >> j) & 1ull)) return C{T(0), T(0)};
       const T kw = sl.ky[th.ra] * sl.kz[dz];
       P sr0 = Ops::zero(), sr1 = Ops::zero(), si0 = Ops::zero(), si1 = Ops::zero();
 #pragma unroll
@@ -851,7 +859,7 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
 #pragma unroll
         for (int kk = 0; kk < G; ++kk) {
           const int j = j0 + kk;
-          red[th.warp][kk][th.lane] = j < nb ? partial(sb[j], sb[j].lyp) : C{T(0), T(0)};
+          red[th.warp][kk][th.lane] = j < nb ? partial(sb[j], j) : C{T(0), T(0)};
         }
       } else {
 #pragma unroll 1
@@ -883,7 +891,7 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
               dz = (th.rb - cur) & (S::RZ - 1);
               if (dz == 0) prefetch(cur + S::RZ);
             }
-            part = partial(sl, lyp);
+            part = partial(sl, j);
           }
           red[th.warp][kk][th.lane] = part;
         }
