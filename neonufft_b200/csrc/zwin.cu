@@ -833,8 +833,8 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
       const u32 bits = __ballot_sync(0xffffffffu, j < nb && th.owns(sb[j < nb ? j : 0].lyp & 15));
       own |= (unsigned long long)bits << (32 * h);
     }
-    auto partial = [&](const Slot& sl, int j) -> C {
-      if (!((own >> j) & 1ull)) return C{T(0), T(0)};
+    // Row sum of an owned point over this thread's row, times ky kz.
+    auto partial = [&](const Slot& sl) -> C {
       const T kw = sl.ky[th.ra] * sl.kz[dz];
       P sr0 = Ops::zero(), sr1 = Ops::zero(), si0 = Ops::zero(), si1 = Ops::zero();
 #pragma unroll
@@ -855,11 +855,13 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
     for (int j0 = 0; j0 < nb; j0 += G) {
       // Points are plane-sorted: if the group's last point is on the window's first plane, so
       // are all of them and the window does not move inside the group.
+      // ownership bits of the group (bit kk: slot j0 + kk); zero past the batch's points
+      const u32 ob = u32(own >> j0);
       if ((sb[min(j0 + G, nb) - 1].lyp >> 4) == cur) {
+        const Slot* g0 = sb + j0;
 #pragma unroll
         for (int kk = 0; kk < G; ++kk) {
-          const int j = j0 + kk;
-          red[th.warp][kk][th.lane] = j < nb ? partial(sb[j], j) : C{T(0), T(0)};
+          red[th.warp][kk][th.lane] = ((ob >> kk) & 1u) ? partial(g0[kk]) : C{T(0), T(0)};
         }
       } else {
 #pragma unroll 1
@@ -891,7 +893,7 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
               dz = (th.rb - cur) & (S::RZ - 1);
               if (dz == 0) prefetch(cur + S::RZ);
             }
-            part = partial(sl, j);
+            if ((ob >> kk) & 1u) part = partial(sl);
           }
           red[th.warp][kk][th.lane] = part;
         }
