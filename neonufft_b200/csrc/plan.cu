@@ -160,7 +160,7 @@ public:
   }
 
   bool fused_key(int* key) const override {
-    if (method_ != 3 || dim_ != 3 || points_.size() == 0) return false;
+    if (method_ != 3 || dim_ != 3 || points_.size() == 0 || tile_[1] != 8) return false;
     *key = kp_.w | (tile_[0] << 8);
     return true;
   }

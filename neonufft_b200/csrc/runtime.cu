@@ -277,13 +277,20 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
     // precisions (3D w = 8 FP32 spreading 2.58 against 2.76 ms at M = 1e7, 24.6 against 25.8 ms
     // at M = 1e8, interpolation unchanged).
     tile[0] = 4;
+    tile[1] = 8;
     if (explicit_tile) {
       if (requested[0] != 2 && requested[0] != 4 && requested[0] != 8) {
         throw_input("spread method 3 supports tiles of 2, 4 or 8 cells in x");
       }
       tile[0] = requested[0];
+      if (requested[1] == 16) {
+        // 16-row tiles (6 warps per CTA) are built for single precision only
+        if (complex_bytes != 8) throw_input("spread method 3 uses 16-row tiles in single precision only");
+        tile[1] = 16;
+      } else if (requested[1] != 0 && requested[1] != 8) {
+        throw_input("spread method 3 supports tiles of 8 or 16 rows");
+      }
     }
-    tile[1] = 8;
     tile[2] = 1;
     return;
   }

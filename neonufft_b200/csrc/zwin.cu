@@ -25,7 +25,7 @@
 //  * when the next point starts on a later plane, the window advances: spreading adds each
 //    completed plane to the fine grid (float2 / double2 atomics: neighbouring columns and
 //    chunks overlap by the halo); interpolation reloads the threads that held it with the
-//    plane RZ further on, prefetched with cp.async one plane ahead;
+//    plane RZ further on (plain loads: a cp.async prefetch one plane ahead measured no faster);
 //  * interpolation reduces the row sums of eight points at a time through a per-warp
 //    shared-memory transpose, then over warps.
 #include <type_traits>
@@ -109,35 +109,39 @@ __device__ __forceinline__ void atomic_add_cplx(double2* p, double2 v) {
 }
 
 // ---- geometry ----------------------------------------------------------------------------------
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY_ = 8>
 struct ZShape {
   static constexpr int RZ = W <= 4 ? 4 : 8;         // window planes = z residues (>= W)
   static constexpr int LA = 32 / RZ;                // rows per warp
-  static constexpr int RY = 16;                     // region rows (>= P1)
+  static constexpr int TY = TY_;                    // tile y (8 or 16)
+  static constexpr int RY = TY + 8;                 // region rows (>= P1)
   static constexpr int NWARP = RY / LA;
   static constexpr int NT = 32 * NWARP;             // threads per CTA
-  static constexpr int TY = 8;                      // tile y
   static constexpr int P0 = TX + W - 1;             // region x extent (cells)
   static constexpr int NP = (P0 + 1) / 2;           // cell pairs per row
   static constexpr int KXN = 4 * ((NP + 1) / 2);    // staged kx values (16-byte multiple)
   static constexpr int P1 = TY + W - 1;             // region y extent
-  static constexpr int BATCH = sizeof(T) == 4 ? 64 : 32;  // points staged at a time
+  // points staged at a time: a multiple of the warps (each stages its share)
+  static constexpr int BATCH = sizeof(T) == 4 ? (NWARP % 3 == 0 ? 48 : 64) : 32;
   static constexpr int G = 8;                       // points reduced together (interpolation)
   // CTAs per SM the interpolation kernel is compiled for: uncapped, it took 96 registers and
   // spilled; capped at 5, 87 (float) / 96 (double) registers without spills, 3 % faster.
   static constexpr int INTERP_CTAS = 5;
-  // CTAs per SM the persistent kernels are compiled for: without the cap, their loop over items
-  // lets the register allocator grow far past the per-transform kernels (166 against 72).
-  static constexpr int SPREAD_FUSED_CTAS = sizeof(T) == 4 ? 7 : 4;
-  static constexpr int INTERP_FUSED_CTAS = sizeof(T) == 4 ? 6 : 4;
   static_assert(W <= RZ && P1 <= RY, "window smaller than the kernel footprint");
   static_assert(BATCH % NWARP == 0 && BATCH / NWARP <= 32, "staging threads");
 };
 
+// CTAs per SM the persistent kernels are compiled for: without the cap, their loop over items
+// lets the register allocator grow far past the per-transform kernels (166 against 72).
+template <typename T>
+constexpr int kSpreadFusedCtas = sizeof(T) == 4 ? 7 : 4;
+template <typename T>
+constexpr int kInterpFusedCtas = sizeof(T) == 4 ? 6 : 4;
+
 // Per-point data staged in shared memory (one slot per point of a batch).
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 struct alignas(16) ZSlotFields {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   T kx[S::KXN];    // kx over the region's x range, zero outside the footprint
   T ky[S::RY];     // ky over the region rows, zero outside the footprint
   T kz[S::RZ];     // kz per window offset, zero beyond w
@@ -153,20 +157,20 @@ struct ZSlotPad {
 };
 template <>
 struct ZSlotPad<true> {};
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 struct alignas(16) ZSlot
-    : ZSlotFields<T, W, TX>, ZSlotPad<(sizeof(ZSlotFields<T, W, TX>) / 16) % 2 == 1> {};
+    : ZSlotFields<T, W, TX, TY>, ZSlotPad<(sizeof(ZSlotFields<T, W, TX, TY>) / 16) % 2 == 1> {};
 
 // Stages `count` (<= 16) bin-sorted records `recs` into slots[0 .. count), one warp: lanes
 // 0 .. count - 1 load the records (and, for spreading, the strengths); then lane pair
 // (2p, 2p + 1) fills point p's slot with the same instruction stream: the even lane kx and the
 // first half of kz, the odd lane ky and the second half, each zeroing half of the contiguous
 // kx / ky arrays first, so all 32 lanes evaluate kernel values.
-template <typename T, int W, int TX, bool SPREAD>
-__device__ __forceinline__ void stage_warp(ZSlot<T, W, TX>* slots, const PointRec<T>* recs,
+template <typename T, int W, int TX, bool SPREAD, int TY = 8>
+__device__ __forceinline__ void stage_warp(ZSlot<T, W, TX, TY>* slots, const PointRec<T>* recs,
                                            int count, const cplx_t<T>* in,
                                            const cplx_t<T>* prephase, T beta, T c, int lane) {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   using C = cplx_t<T>;
   constexpr unsigned kFull = 0xffffffffu;
   PointRec<T> rec;
@@ -190,7 +194,7 @@ __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX>* slots, const PointRe
   const T fz = __shfl_sync(kFull, rec.frac[2], p);
   const T vx = __shfl_sync(kFull, v.x, p);
   const T vy = __shfl_sync(kFull, v.y, p);
-  ZSlot<T, W, TX>& sl = slots[p < count ? p : 0];
+  ZSlot<T, W, TX, TY>& sl = slots[p < count ? p : 0];
   constexpr int kZero16 = int((S::KXN + S::RY) * sizeof(T) / 16);  // kx and ky are contiguous
   constexpr int kHalf = (kZero16 + 1) / 2;
   if (p < count) {
@@ -280,9 +284,9 @@ __device__ __forceinline__ bool zcta(const BinGeom& g, const u32* bin_start, ZCh
 }
 
 // Thread layout shared by both kernels.
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 struct ZThread {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   int tid, warp, lane, ra, rb, a_lo;
   int stage_j;  // batch slot this thread stages (< BATCH), or -1
   __device__ __forceinline__ ZThread() {
@@ -301,27 +305,27 @@ struct ZThread {
 };
 
 // ---- spreading ---------------------------------------------------------------------------------
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 struct ZSpreadShared {
-  ZSlot<T, W, TX> slots[2][ZShape<T, W, TX>::BATCH];
+  ZSlot<T, W, TX, TY> slots[2][ZShape<T, W, TX, TY>::BATCH];
 };
 
 // Spreads work item `item` of batch entry `batch` (one CTA; every thread calls it).
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks ch,
                                                  const WorkList& wl, u32 item, int batch,
-                                                 ZSpreadShared<T, W, TX>& sh) {
-  using S = ZShape<T, W, TX>;
+                                                 ZSpreadShared<T, W, TX, TY>& sh) {
+  using S = ZShape<T, W, TX, TY>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  using Slot = ZSlot<T, W, TX>;
+  using Slot = ZSlot<T, W, TX, TY>;
   auto& slots = sh.slots;
 
   const BinGeom& g = a.g;
   ZCta cta;
   if (!zcta(g, a.pts.bin_start, ch, wl, item, cta)) return;
-  const ZThread<T, W, TX> th;
+  const ZThread<T, W, TX, TY> th;
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
@@ -379,7 +383,7 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
     constexpr int PW = S::BATCH / S::NWARP;  // points per warp
     const int count = min(nb - th.warp * PW, PW);
     for (int c0 = 0; c0 < count; c0 += 16) {
-      stage_warp<T, W, TX, true>(slots[k & 1] + th.warp * PW + c0,
+      stage_warp<T, W, TX, true, TY>(slots[k & 1] + th.warp * PW + c0,
                                  a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
                                  min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane);
     }
@@ -394,14 +398,14 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
     const Slot* sb = slots[k & 1];
     // The points of this batch whose footprint covers rows of this warp, one bit per slot: the
     // warp visits only those, with a window of its own (no other warp touches its rows).
-    u32 own[S::BATCH / 32];
+    u32 own[(S::BATCH + 31) / 32];
 #pragma unroll
-    for (int h = 0; h < S::BATCH / 32; ++h) {
+    for (int h = 0; h < (S::BATCH + 31) / 32; ++h) {
       const int j = h * 32 + th.lane;
       own[h] = __ballot_sync(0xffffffffu, j < nb && th.owns(sb[j < nb ? j : 0].lyp & 15));
     }
 #pragma unroll
-    for (int h = 0; h < S::BATCH / 32; ++h) {
+    for (int h = 0; h < (S::BATCH + 31) / 32; ++h) {
       for (u32 m = own[h]; m != 0u; m &= m - 1u) {
         const Slot& sl = sb[h * 32 + __ffs(int(m)) - 1];
         const int tp = sl.lyp >> 4;
@@ -438,12 +442,12 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
   flush(cur + ((th.rb - cur) & (S::RZ - 1)));  // the rest of the window
 }
 
-template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT)
+template <typename T, int W, int TX, int TY>
+__global__ void __launch_bounds__(ZShape<T, W, TX, TY>::NT)
     spread_zwin_kernel(const __grid_constant__ SpreadArgs<T> a, ZChunks ch,
                        const __grid_constant__ WorkList wl) {
-  __shared__ ZSpreadShared<T, W, TX> sh;
-  spread_zwin_item<T, W, TX>(a, ch, wl, blockIdx.x, int(blockIdx.y), sh);
+  __shared__ ZSpreadShared<T, W, TX, TY> sh;
+  spread_zwin_item<T, W, TX, TY>(a, ch, wl, blockIdx.x, int(blockIdx.y), sh);
 }
 
 // Takes the next item of the queue spanning all jobs; every thread returns the same values.
@@ -481,7 +485,7 @@ __device__ __forceinline__ bool next_fused_item(const Job* jobs, const i64* item
 }
 
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::SPREAD_FUSED_CTAS)
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, kSpreadFusedCtas<T>)
     spread_zwin_fused_kernel(const ZSpreadJob<T>* jobs, const i64* item_end, int njobs,
                              i64 total, u32* queue) {
   __shared__ ZSpreadShared<T, W, TX> sh;
@@ -669,60 +673,40 @@ __global__ void __launch_bounds__(128) spread_zmma_kernel(SpreadArgs<float> a, Z
 }
 
 // ---- interpolation -----------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async_cell(void* smem, const float2* g) {
-  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_cell(void* smem, const double2* g) {
-  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_16(void* smem, const void* g) {
-  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 struct ZInterpShared {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   static constexpr int RS = 33;  // odd row stride of the transpose buffer: conflict-free reads
-  ZSlot<T, W, TX> slots[2][S::BATCH];
+  ZSlot<T, W, TX, TY> slots[2][S::BATCH];
   cplx_t<T> red[S::NWARP][S::G][RS];
   cplx_t<T> res[2][S::NWARP][S::BATCH];
-  cplx_t<T> stage_row[S::RY][2 * S::NP];  // next plane of the loading threads' rows
 };
 
 // Interpolates work item `item` (one CTA; every thread calls it).
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY = 8>
 __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks ch,
                                                  const WorkList& wl, u32 item,
-                                                 ZInterpShared<T, W, TX>& sh) {
-  using S = ZShape<T, W, TX>;
+                                                 ZInterpShared<T, W, TX, TY>& sh) {
+  using S = ZShape<T, W, TX, TY>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
   using C = cplx_t<T>;
-  using Slot = ZSlot<T, W, TX>;
+  using Slot = ZSlot<T, W, TX, TY>;
   constexpr int G = S::G;
   auto& slots = sh.slots;
   auto& red = sh.red;
   auto& res = sh.res;
-  auto& stage_row = sh.stage_row;
 
   const BinGeom& g = a.g;
   ZCta cta;
   if (!zcta(g, a.pts.bin_start, ch, wl, item, cta)) return;
-  const ZThread<T, W, TX> th;
+  const ZThread<T, W, TX, TY> th;
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
   const bool narrow = nfx < S::P0;
   const bool has_row = th.ra < S::P1;
   const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
   const i64 gx0 = i64(cta.tx) * TX;
-  if (th.tid < S::RY) {
-    for (int i = S::P0; i < 2 * S::NP; ++i) stage_row[th.tid][i] = C{T(0), T(0)};  // padding
-  }
 
   // Row values of the window plane: real / imaginary parts of cell pairs (2q, 2q + 1); rows
   // outside the region stay zero.
@@ -731,7 +715,6 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
   for (int q = 0; q < S::NP; ++q) gre[q] = gim[q] = Ops::zero();
   // The region's x range lies inside the grid (the usual case): contiguous row segments.
   const bool contiguous = !narrow && gx0 + S::P0 <= nfx;
-  const bool pairs16 = contiguous && (nfx % 2) == 0 && (reinterpret_cast<size_t>(grid) % 16) == 0;
   auto load_row = [&](int p) {
     if (!has_row) return;
     const C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
@@ -749,41 +732,6 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
       gim[q] = Ops::pack(c0.y, c1.y);
     }
   };
-  bool pending = false;  // a cp.async of this thread's next plane is in flight
-  auto prefetch = [&](int p) {
-    if (!has_row) return;
-    const C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
-    if (pairs16 && sizeof(T) == 4) {
-      // 16-byte copies of cell pairs (the stage rows are 16-byte aligned)
-#pragma unroll
-      for (int q = 0; q < S::NP; ++q) {
-        if (2 * q + 1 < S::P0) {
-          cp_async_16(&stage_row[th.ra][2 * q], row + gx0 + 2 * q);
-        } else {
-          cp_async_cell(&stage_row[th.ra][2 * q], row + gx0 + 2 * q);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < S::P0; ++i) {
-        cp_async_cell(&stage_row[th.ra][i], row + wrap_x(gx0, i, nfx, narrow));
-      }
-    }
-    cp_async_commit();
-    pending = true;
-  };
-  auto take_prefetched = [&]() {
-    cp_async_wait_all();
-    pending = false;
-#pragma unroll
-    for (int q = 0; q < S::NP; ++q) {
-      const C c0 = stage_row[th.ra][2 * q];
-      const C c1 = stage_row[th.ra][2 * q + 1];
-      gre[q] = Ops::pack(c0.x, c1.x);
-      gim[q] = Ops::pack(c0.y, c1.y);
-    }
-  };
-
   const u32 npts = cta.pend - cta.pbeg;
   const int nbatch = int((npts + S::BATCH - 1) / S::BATCH);
   auto stage = [&](int k) {
@@ -792,7 +740,7 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
     constexpr int PW = S::BATCH / S::NWARP;  // points per warp
     const int count = min(nb - th.warp * PW, PW);
     for (int c0 = 0; c0 < count; c0 += 16) {
-      stage_warp<T, W, TX, false>(slots[k & 1] + th.warp * PW + c0,
+      stage_warp<T, W, TX, false, TY>(slots[k & 1] + th.warp * PW + c0,
                                   a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
                                   min(count - c0, 16), nullptr, nullptr, a.beta, a.c, th.lane);
     }
@@ -820,7 +768,6 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
   int cur = slots[0][0].lyp >> 4;  // window start: the first point's plane
   int dz = (th.rb - cur) & (S::RZ - 1);
   load_row(cur + dz);
-  if (dz == 0) prefetch(cur + S::RZ);
 
   for (int k = 0; k < nbatch; ++k) {
     const int nb = int(min(npts - u32(k) * S::BATCH, u32(S::BATCH)));
@@ -874,24 +821,14 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
             const int tp = lyp >> 4;
             if (tp != cur) {  // advance the window: rows of planes [cur, tp) move on by RZ
               if (tp - cur >= S::RZ) {
-                if (pending) cp_async_wait_all();
-                pending = false;
                 load_row(tp + ((th.rb - tp) & (S::RZ - 1)));
               } else {
                 for (int i = 0; i < tp - cur; ++i) {
-                  if (th.rb == ((cur + i) & (S::RZ - 1))) {
-                    if (pending) {
-                      take_prefetched();
-                    } else {
-                      load_row(cur + i + S::RZ);
-                    }
-                  }
+                  if (th.rb == ((cur + i) & (S::RZ - 1))) load_row(cur + i + S::RZ);
                 }
               }
-              __syncwarp();  // the staged rows are read before the next prefetch rewrites them
               cur = tp;
               dz = (th.rb - cur) & (S::RZ - 1);
-              if (dz == 0) prefetch(cur + S::RZ);
             }
             if ((ob >> kk) & 1u) part = partial(sl);
           }
@@ -924,19 +861,18 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
     __syncthreads();
   }
   output(nbatch - 1);
-  if (pending) cp_async_wait_all();
 }
 
-template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::INTERP_CTAS)
+template <typename T, int W, int TX, int TY>
+__global__ void __launch_bounds__(ZShape<T, W, TX, TY>::NT, ZShape<T, W, TX, TY>::INTERP_CTAS)
     interp_zwin_kernel(const __grid_constant__ InterpArgs<T> a, ZChunks ch,
                        const __grid_constant__ WorkList wl) {
-  __shared__ ZInterpShared<T, W, TX> sh;
-  interp_zwin_item<T, W, TX>(a, ch, wl, blockIdx.x, sh);
+  __shared__ ZInterpShared<T, W, TX, TY> sh;
+  interp_zwin_item<T, W, TX, TY>(a, ch, wl, blockIdx.x, sh);
 }
 
 template <typename T, int W, int TX>
-__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, ZShape<T, W, TX>::INTERP_FUSED_CTAS)
+__global__ void __launch_bounds__(ZShape<T, W, TX>::NT, kInterpFusedCtas<T>)
     interp_zwin_fused_kernel(const ZInterpJob<T>* jobs, const i64* item_end, int njobs,
                              i64 total, u32* queue) {
   __shared__ ZInterpShared<T, W, TX> sh;
@@ -988,59 +924,59 @@ WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch
   return wl;
 }
 
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY>
 void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
   dim3 grid{unsigned(wl.grid), unsigned(a.batch), 1u};
-  spread_zwin_kernel<T, W, TX><<<grid, S::NT, 0, stream>>>(a, ch, wl);
+  spread_zwin_kernel<T, W, TX, TY><<<grid, S::NT, 0, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();
 }
 
-template <typename T, int W, int TX>
+template <typename T, int W, int TX, int TY>
 void launch_interp_zwin_tw(const InterpArgs<T>& a, cudaStream_t stream) {
-  using S = ZShape<T, W, TX>;
+  using S = ZShape<T, W, TX, TY>;
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
-  interp_zwin_kernel<T, W, TX><<<unsigned(wl.grid), S::NT, 0, stream>>>(a, ch, wl);
+  interp_zwin_kernel<T, W, TX, TY><<<unsigned(wl.grid), S::NT, 0, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();
 }
 
-template <typename T, int TX>
+template <typename T, int TX, int TY>
 void spread_zwin_tx(const SpreadArgs<T>& a, cudaStream_t stream) {
   switch (a.g.w) {
-    case 2: return launch_spread_zwin_tw<T, 2, TX>(a, stream);
-    case 3: return launch_spread_zwin_tw<T, 3, TX>(a, stream);
-    case 4: return launch_spread_zwin_tw<T, 4, TX>(a, stream);
-    case 5: return launch_spread_zwin_tw<T, 5, TX>(a, stream);
-    case 6: return launch_spread_zwin_tw<T, 6, TX>(a, stream);
-    case 7: return launch_spread_zwin_tw<T, 7, TX>(a, stream);
-    case 8: return launch_spread_zwin_tw<T, 8, TX>(a, stream);
+    case 2: return launch_spread_zwin_tw<T, 2, TX, TY>(a, stream);
+    case 3: return launch_spread_zwin_tw<T, 3, TX, TY>(a, stream);
+    case 4: return launch_spread_zwin_tw<T, 4, TX, TY>(a, stream);
+    case 5: return launch_spread_zwin_tw<T, 5, TX, TY>(a, stream);
+    case 6: return launch_spread_zwin_tw<T, 6, TX, TY>(a, stream);
+    case 7: return launch_spread_zwin_tw<T, 7, TX, TY>(a, stream);
+    case 8: return launch_spread_zwin_tw<T, 8, TX, TY>(a, stream);
     default: throw_internal("z-window kernels need n_spread <= 8");
   }
 }
 
-template <typename T, int TX>
+template <typename T, int TX, int TY>
 void interp_zwin_tx(const InterpArgs<T>& a, cudaStream_t stream) {
   switch (a.g.w) {
-    case 2: return launch_interp_zwin_tw<T, 2, TX>(a, stream);
-    case 3: return launch_interp_zwin_tw<T, 3, TX>(a, stream);
-    case 4: return launch_interp_zwin_tw<T, 4, TX>(a, stream);
-    case 5: return launch_interp_zwin_tw<T, 5, TX>(a, stream);
-    case 6: return launch_interp_zwin_tw<T, 6, TX>(a, stream);
-    case 7: return launch_interp_zwin_tw<T, 7, TX>(a, stream);
-    case 8: return launch_interp_zwin_tw<T, 8, TX>(a, stream);
+    case 2: return launch_interp_zwin_tw<T, 2, TX, TY>(a, stream);
+    case 3: return launch_interp_zwin_tw<T, 3, TX, TY>(a, stream);
+    case 4: return launch_interp_zwin_tw<T, 4, TX, TY>(a, stream);
+    case 5: return launch_interp_zwin_tw<T, 5, TX, TY>(a, stream);
+    case 6: return launch_interp_zwin_tw<T, 6, TX, TY>(a, stream);
+    case 7: return launch_interp_zwin_tw<T, 7, TX, TY>(a, stream);
+    case 8: return launch_interp_zwin_tw<T, 8, TX, TY>(a, stream);
     default: throw_internal("z-window kernels need n_spread <= 8");
   }
 }
 
 void check_zwin_geom(const BinGeom& g) {
-  if (g.dim != 3 || !g.zmajor || g.tile[1] != 8 || g.tile[2] != 1 ||
+  if (g.dim != 3 || !g.zmajor || (g.tile[1] != 8 && g.tile[1] != 16) || g.tile[2] != 1 ||
       (g.tile[0] != 2 && g.tile[0] != 4 && g.tile[0] != 8) || g.w > 8) {
-    throw_internal("z-window kernels need a 3D plane-major (4|8, 8, 1) tiling and n_spread <= 8");
+    throw_internal("z-window kernels need a 3D plane-major (2|4|8, 8|16, 1) tiling and n_spread <= 8");
   }
 }
 
@@ -1129,22 +1065,39 @@ void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream) {
     }
     throw_internal("tensor-core spreading is single precision");
   }
-  if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8>(a, stream);
-  if (a.g.tile[0] == 2) return spread_zwin_tx<T, 2>(a, stream);
-  return spread_zwin_tx<T, 4>(a, stream);
+  if (a.g.tile[1] == 16) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8, 16>(a, stream);
+      if (a.g.tile[0] == 2) return spread_zwin_tx<T, 2, 16>(a, stream);
+      return spread_zwin_tx<T, 4, 16>(a, stream);
+    }
+    throw_internal("z-window tiles of 16 rows are single precision");
+  }
+  if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8, 8>(a, stream);
+  if (a.g.tile[0] == 2) return spread_zwin_tx<T, 2, 8>(a, stream);
+  return spread_zwin_tx<T, 4, 8>(a, stream);
 }
 
 template <typename T>
 void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream) {
   check_zwin_geom(a.g);
-  if (a.g.tile[0] == 8) return interp_zwin_tx<T, 8>(a, stream);
-  if (a.g.tile[0] == 2) return interp_zwin_tx<T, 2>(a, stream);
-  return interp_zwin_tx<T, 4>(a, stream);
+  if (a.g.tile[1] == 16) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.g.tile[0] == 8) return interp_zwin_tx<T, 8, 16>(a, stream);
+      if (a.g.tile[0] == 2) return interp_zwin_tx<T, 2, 16>(a, stream);
+      return interp_zwin_tx<T, 4, 16>(a, stream);
+    }
+    throw_internal("z-window tiles of 16 rows are single precision");
+  }
+  if (a.g.tile[0] == 8) return interp_zwin_tx<T, 8, 8>(a, stream);
+  if (a.g.tile[0] == 2) return interp_zwin_tx<T, 2, 8>(a, stream);
+  return interp_zwin_tx<T, 4, 8>(a, stream);
 }
 
 template <typename T>
 ZSpreadJob<T> zwin_spread_job(const SpreadArgs<T>& a) {
   check_zwin_geom(a.g);
+  if (a.g.tile[1] != 8) throw_internal("persistent z-window kernels use tiles of 8 rows");
   if (a.method != 3 || a.batch != 1) throw_internal("persistent spreading is method 3, batch 1");
   ZSpreadJob<T> j;
   j.a = a;
@@ -1156,6 +1109,7 @@ ZSpreadJob<T> zwin_spread_job(const SpreadArgs<T>& a) {
 template <typename T>
 ZInterpJob<T> zwin_interp_job(const InterpArgs<T>& a) {
   check_zwin_geom(a.g);
+  if (a.g.tile[1] != 8) throw_internal("persistent z-window kernels use tiles of 8 rows");
   if (a.method != 3) throw_internal("persistent interpolation is method 3");
   ZInterpJob<T> j;
   j.a = a;

@@ -73,9 +73,12 @@ def test_zwin_matches_slabs_and_direct(dtype, w, type_, cuda, engine, oracle):
 
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("type_", [1, 2])
-@pytest.mark.parametrize("method", [1, 2, 3])
-def test_clustered_points(dtype, type_, method, cuda, engine, oracle):
+@pytest.mark.parametrize("method,tile", [(1, (0, 0, 0)), (2, (0, 0, 0)), (3, (0, 0, 0)),
+                                         (3, (4, 16, 1))])
+def test_clustered_points(dtype, type_, method, tile, cuda, engine, oracle):
     """500 points inside one tile and plane (several batches of one plane) plus scattered ones."""
+    if tile[1] == 16 and dtype == "float64":
+        pytest.skip("16-row tiles are single precision")
     rng = np.random.default_rng(7 + type_)
     modes = [24, 24, 24]
     M0, M1 = 500, 300
@@ -88,7 +91,7 @@ def test_clustered_points(dtype, type_, method, cuda, engine, oracle):
     inp = rng.standard_normal(n_in) + 1j * rng.standard_normal(n_in)
     tol = 1e-5 if dtype == "float32" else 1e-7  # kernel widths 6 and 8
     out, info = run_t12(engine, cuda, dtype, 1, pts, inp, modes, type_, tol=tol,
-                        spread_method=method)
+                        spread_method=method, tile=tile)
     assert info["spread_method"] == method
     ref = direct(oracle, type_, 1, pts, inp, modes, dtype)
     bound = 3e-5 if dtype == "float32" else 1e-6
@@ -98,9 +101,11 @@ def test_clustered_points(dtype, type_, method, cuda, engine, oracle):
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("w", [2, 8])
 @pytest.mark.parametrize("type_", [1, 2])
-@pytest.mark.parametrize("tx", [2, 4, 8])
-def test_zwin_tiny_grid(dtype, w, type_, tx, cuda, engine, oracle):
+@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (4, 16)])
+def test_zwin_tiny_grid(dtype, w, type_, tx, ty, cuda, engine, oracle):
     """Fine grids of 2w cells per dimension: the tile's halo region wraps around the grid."""
+    if ty == 16 and dtype == "float64":
+        pytest.skip("16-row tiles are single precision")
     rng = np.random.default_rng(3 * w + type_)
     modes = [3, 2, 4]
     M = 200
@@ -108,7 +113,7 @@ def test_zwin_tiny_grid(dtype, w, type_, tx, cuda, engine, oracle):
     n_in = M if type_ == 1 else int(np.prod(modes))
     inp = rng.standard_normal(n_in) + 1j * rng.standard_normal(n_in)
     out3, _ = run_t12(engine, cuda, dtype, -1, pts, inp, modes, type_, n_spread=w,
-                      spread_method=3, tile=(tx, 8, 1))
+                      spread_method=3, tile=(tx, ty, 1))
     out1, _ = run_t12(engine, cuda, dtype, -1, pts, inp, modes, type_, n_spread=w,
                       spread_method=1)
     ref = direct(oracle, type_, -1, pts, inp, modes, dtype)
@@ -117,8 +122,10 @@ def test_zwin_tiny_grid(dtype, w, type_, tx, cuda, engine, oracle):
 
 
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
-@pytest.mark.parametrize("tx", [2, 4, 8])
-def test_zwin_tile_widths(dtype, tx, cuda, engine, oracle):
+@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (2, 16), (4, 16), (8, 16)])
+def test_zwin_tile_widths(dtype, tx, ty, cuda, engine, oracle):
+    if ty == 16 and dtype == "float64":
+        pytest.skip("16-row tiles are single precision")
     rng = np.random.default_rng(tx)
     modes = [33, 20, 18]
     M = 4000
@@ -127,10 +134,10 @@ def test_zwin_tile_widths(dtype, tx, cuda, engine, oracle):
     f = rng.standard_normal(int(np.prod(modes))) + 1j * rng.standard_normal(int(np.prod(modes)))
     tol = 1e-6 if dtype == "float32" else 1e-7
     o1, info = run_t12(engine, cuda, dtype, -1, pts, c, modes, 1, tol=tol, spread_method=3,
-                       tile=(tx, 8, 1))
+                       tile=(tx, ty, 1))
     o2, _ = run_t12(engine, cuda, dtype, 1, pts, f, modes, 2, tol=tol, spread_method=3,
-                    tile=(tx, 8, 1))
-    assert list(info["tile"]) == [tx, 8, 1]
+                    tile=(tx, ty, 1))
+    assert list(info["tile"]) == [tx, ty, 1]
     bound = 2e-5 if dtype == "float32" else 1e-6
     assert oracle.rel_l2(o1, direct(oracle, 1, -1, pts, c, modes, dtype)) < bound
     assert oracle.rel_l2(o2, direct(oracle, 2, 1, pts, f, modes, dtype)) < bound
