@@ -66,7 +66,7 @@ WORKLOADS = {
 # of the same configuration (profiles/zwin_c2.md): (workload, precision, method, n_spread, tile,
 # kernel) -> bytes per point.
 DRAM_BYTES_PER_POINT = {
-    ("c2", "f32", 3, 8, (4, 8, 1), "interp"): (672.003840e6 + 263.595776e6) / 1e7,
+    ("c2", "f32", 3, 8, (4, 8, 1), "interp"): (669.191936e6 + 261.929472e6) / 1e7,
     ("c2", "f32", 3, 8, (4, 8, 1), "spread"): (959.445760e6 + 144.172288e6) / 1e7,
     ("c2", "f32", 3, 8, (8, 8, 1), "interp"): (665.430528e6 + 261.607424e6) / 1e7,
     ("c2", "f32", 3, 8, (8, 8, 1), "spread"): (943.662592e6 + 131.524864e6) / 1e7,
