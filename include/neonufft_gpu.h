@@ -56,8 +56,14 @@ typedef struct NnbOptions {
   int kernel_approximation; /* ignored: the ES kernel is always evaluated directly */
   int order;                /* NeonufftModeOrder */
   int kernel_type;          /* NeonufftKernelType */
-  int tile[3];              /* subproblem tile (bin) shape in fine-grid cells; 0 = automatic */
-  int spread_method;        /* 0 = automatic; 1 = warp-private slabs; 2 = thread per point */
+  int tile[3];              /* subproblem tile (bin) shape in fine-grid cells; 0 = automatic.
+                               Method 3 takes {2|4|8, 8|16, 1} (16 rows: single precision);
+                               the default is {4, 8, 1} */
+  int spread_method;        /* 0 = automatic (3 for 3D plans with kernel width <= 8, else 1);
+                               1 = warp-private shared-memory slabs; 2 = thread per point;
+                               3 = sliding z-window held in registers (3D, width <= 8);
+                               4 = method 3 with the row updates on the tensor cores (TF32 with
+                               split operands; 3D, single precision, width 5 to 8) */
   int n_spread;             /* kernel width override in [2, 16]; 0 = the reference heuristic */
   int reserved[7];
 } NnbOptions;

@@ -80,7 +80,7 @@ struct SpreadArgs {
   int batch;
   T beta;
   T c;
-  int method;  // 1: warp-private slabs, 2: thread per point, 3: z-window (zwin.cu)
+  int method;  // 1: warp-private slabs, 2: thread per point, 3: z-window, 4: z-window on tensor cores (zwin.cu)
 };
 template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream);
