@@ -287,8 +287,14 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
         // 16-row tiles (6 warps per CTA) are built for single precision only
         if (complex_bytes != 8) throw_input("spread method 3 uses 16-row tiles in single precision only");
         tile[1] = 16;
+      } else if (requested[1] == 4) {
+        // 4-row tiles (3 warps per CTA): single precision, 4 cells in x
+        if (complex_bytes != 8 || tile[0] != 4) {
+          throw_input("spread method 3 uses 4-row tiles in single precision with 4 cells in x");
+        }
+        tile[1] = 4;
       } else if (requested[1] != 0 && requested[1] != 8) {
-        throw_input("spread method 3 supports tiles of 8 or 16 rows");
+        throw_input("spread method 3 supports tiles of 4, 8 or 16 rows");
       }
     }
     tile[2] = 1;

@@ -113,16 +113,18 @@ template <typename T, int W, int TX, int TY_ = 8>
 struct ZShape {
   static constexpr int RZ = W <= 4 ? 4 : 8;         // window planes = z residues (>= W)
   static constexpr int LA = 32 / RZ;                // rows per warp
-  static constexpr int TY = TY_;                    // tile y (8 or 16)
-  static constexpr int RY = TY + 8;                 // region rows (>= P1)
+  static constexpr int TY = TY_;                    // tile y (4, 8 or 16)
+  static constexpr int P1 = TY + W - 1;             // region y extent
+  // region rows (>= P1, a multiple of the rows per warp)
+  static constexpr int RY = TY == 4 ? (P1 + LA - 1) / LA * LA : TY + 8;
   static constexpr int NWARP = RY / LA;
   static constexpr int NT = 32 * NWARP;             // threads per CTA
   static constexpr int P0 = TX + W - 1;             // region x extent (cells)
   static constexpr int NP = (P0 + 1) / 2;           // cell pairs per row
   static constexpr int KXN = 4 * ((NP + 1) / 2);    // staged kx values (16-byte multiple)
-  static constexpr int P1 = TY + W - 1;             // region y extent
   // points staged at a time: a multiple of the warps (each stages its share)
-  static constexpr int BATCH = sizeof(T) == 4 ? (NWARP % 3 == 0 ? 48 : 64) : 32;
+  static constexpr int BATCH =
+      sizeof(T) == 4 ? (NWARP == 1 ? 32 : (NWARP % 3 == 0 ? 48 : 64)) : 32;
   static constexpr int G = 8;                       // points reduced together (interpolation)
   // CTAs per SM the interpolation kernel is compiled for: 6 in single precision (78 registers,
   // no spills; 86 uncapped, which allows only 5 CTAs and measured 6 % slower), 5 in double.
@@ -994,9 +996,10 @@ void interp_zwin_tx(const InterpArgs<T>& a, cudaStream_t stream) {
 }
 
 void check_zwin_geom(const BinGeom& g) {
-  if (g.dim != 3 || !g.zmajor || (g.tile[1] != 8 && g.tile[1] != 16) || g.tile[2] != 1 ||
+  if (g.dim != 3 || !g.zmajor || (g.tile[1] != 4 && g.tile[1] != 8 && g.tile[1] != 16) ||
+      g.tile[2] != 1 ||
       (g.tile[0] != 2 && g.tile[0] != 4 && g.tile[0] != 8) || g.w > 8) {
-    throw_internal("z-window kernels need a 3D plane-major (2|4|8, 8|16, 1) tiling and n_spread <= 8");
+    throw_internal("z-window kernels need a 3D plane-major (2|4|8, 4|8|16, 1) tiling and n_spread <= 8");
   }
 }
 
@@ -1093,6 +1096,12 @@ void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream) {
     }
     throw_internal("z-window tiles of 16 rows are single precision");
   }
+  if (a.g.tile[1] == 4) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.g.tile[0] == 4) return spread_zwin_tx<T, 4, 4>(a, stream);
+    }
+    throw_internal("z-window tiles of 4 rows are single precision, 4 cells in x");
+  }
   if (a.g.tile[0] == 8) return spread_zwin_tx<T, 8, 8>(a, stream);
   if (a.g.tile[0] == 2) return spread_zwin_tx<T, 2, 8>(a, stream);
   return spread_zwin_tx<T, 4, 8>(a, stream);
@@ -1108,6 +1117,12 @@ void launch_interp_zwin(const InterpArgs<T>& a, cudaStream_t stream) {
       return interp_zwin_tx<T, 4, 16>(a, stream);
     }
     throw_internal("z-window tiles of 16 rows are single precision");
+  }
+  if (a.g.tile[1] == 4) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.g.tile[0] == 4) return interp_zwin_tx<T, 4, 4>(a, stream);
+    }
+    throw_internal("z-window tiles of 4 rows are single precision, 4 cells in x");
   }
   if (a.g.tile[0] == 8) return interp_zwin_tx<T, 8, 8>(a, stream);
   if (a.g.tile[0] == 2) return interp_zwin_tx<T, 2, 8>(a, stream);

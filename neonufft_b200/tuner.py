@@ -59,11 +59,12 @@ def heuristic_width(tol: float, upsampfac: float, precision: str) -> int:
 
 
 def resolved(p: Problem, c: Config):
-    """(kernel width, method, x tile) that a plan with configuration c uses."""
+    """(kernel width, method, x tile, y tile) that a plan with configuration c uses."""
     w = c.n_spread or heuristic_width(p.tol, c.upsampfac, p.precision)
     method = c.method or (3 if p.dim == 3 and w <= 8 else 1)
     tile0 = c.tile[0] or (4 if method == 3 else 0)
-    return w, method, tile0
+    tile1 = c.tile[1] or (8 if method == 3 else 0)
+    return w, method, tile0, tile1
 
 
 def candidates(p: Problem):
@@ -78,6 +79,8 @@ def candidates(p: Problem):
                 methods = [(1, (0, 0, 0))]
                 if w <= 8:
                     methods = [(3, (8, 8, 1)), (3, (4, 8, 1))] + methods
+                    if p.precision == "f32" and w >= 5:
+                        methods.insert(2, (3, (4, 4, 1)))  # 4-row tiles: single precision
             elif p.dim == 2:
                 methods = [(1, (0, 0, 0)), (2, (0, 0, 0))]
             else:
@@ -90,18 +93,18 @@ def candidates(p: Problem):
 
 
 def features(p: Problem, c: Config) -> np.ndarray:
-    w, method, tile0 = resolved(p, c)
+    w, method, tile0, tile1 = resolved(p, c)
     nf = max(2 * w, int(p.N * c.upsampfac))
     lcells = p.dim * math.log10(nf)
     return np.array([
         float(p.dim == 3), float(p.type == 2), math.log10(p.M), p.dim * math.log10(p.N), lcells,
         -math.log10(p.tol), float(p.precision == "f64"), float(p.blob), c.upsampfac, float(w),
         float(method == 1), float(method == 2), float(method == 3), float(tile0),
-        math.log10(p.M) - lcells, float(w) ** p.dim / 100.0,
+        math.log10(p.M) - lcells, float(w) ** p.dim / 100.0, float(tile1),
     ], dtype=np.float64)
 
 
-N_FEATURES = 16
+N_FEATURES = 17
 
 
 class ProblemData:

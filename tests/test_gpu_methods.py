@@ -74,11 +74,11 @@ def test_zwin_matches_slabs_and_direct(dtype, w, type_, cuda, engine, oracle):
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("type_", [1, 2])
 @pytest.mark.parametrize("method,tile", [(1, (0, 0, 0)), (2, (0, 0, 0)), (3, (0, 0, 0)),
-                                         (3, (4, 16, 1))])
+                                         (3, (4, 16, 1)), (3, (4, 4, 1))])
 def test_clustered_points(dtype, type_, method, tile, cuda, engine, oracle):
     """500 points inside one tile and plane (several batches of one plane) plus scattered ones."""
-    if tile[1] == 16 and dtype == "float64":
-        pytest.skip("16-row tiles are single precision")
+    if tile[1] in (4, 16) and dtype == "float64":
+        pytest.skip("4- and 16-row tiles are single precision")
     rng = np.random.default_rng(7 + type_)
     modes = [24, 24, 24]
     M0, M1 = 500, 300
@@ -101,11 +101,11 @@ def test_clustered_points(dtype, type_, method, tile, cuda, engine, oracle):
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("w", [2, 8])
 @pytest.mark.parametrize("type_", [1, 2])
-@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (4, 16)])
+@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (4, 16), (4, 4)])
 def test_zwin_tiny_grid(dtype, w, type_, tx, ty, cuda, engine, oracle):
     """Fine grids of 2w cells per dimension: the tile's halo region wraps around the grid."""
-    if ty == 16 and dtype == "float64":
-        pytest.skip("16-row tiles are single precision")
+    if ty != 8 and dtype == "float64":
+        pytest.skip("4- and 16-row tiles are single precision")
     rng = np.random.default_rng(3 * w + type_)
     modes = [3, 2, 4]
     M = 200
@@ -122,10 +122,10 @@ def test_zwin_tiny_grid(dtype, w, type_, tx, ty, cuda, engine, oracle):
 
 
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
-@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (2, 16), (4, 16), (8, 16)])
+@pytest.mark.parametrize("tx,ty", [(2, 8), (4, 8), (8, 8), (2, 16), (4, 16), (8, 16), (4, 4)])
 def test_zwin_tile_widths(dtype, tx, ty, cuda, engine, oracle):
-    if ty == 16 and dtype == "float64":
-        pytest.skip("16-row tiles are single precision")
+    if ty != 8 and dtype == "float64":
+        pytest.skip("4- and 16-row tiles are single precision")
     rng = np.random.default_rng(tx)
     modes = [33, 20, 18]
     M = 4000
