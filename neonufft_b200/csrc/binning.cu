@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kBinBlock)
     }
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
-      if (base + u * stride < M) recs[pos[u]] = r[u];
+      if (base + u * stride < M) store_rec(&recs[pos[u]], r[u]);
     }
   }
 }

@@ -139,6 +139,39 @@ struct alignas(16) PointRec {
 static_assert(sizeof(PointRec<float>) == 32 && sizeof(PointRec<double>) == 32,
               "point records are one 32-byte sector");
 
+// Stores a record as one whole 32-byte sector: two 16-byte stores, the single-precision padding
+// written as zeros. A store of the fields alone leaves part of the sector unwritten, and the L2
+// then reads the sector from memory to merge it when it writes it back: for records placed at
+// random, a second 32 bytes of traffic per point.
+__device__ __forceinline__ void store_rec(PointRec<float>* dst, const PointRec<float>& r) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  d[0] = make_uint4(r.perm, r.local, __float_as_uint(r.frac[0]), __float_as_uint(r.frac[1]));
+  d[1] = make_uint4(__float_as_uint(r.frac[2]), 0u, 0u, 0u);
+}
+__device__ __forceinline__ void store_rec(PointRec<double>* dst, const PointRec<double>& r) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  d[0] = make_uint4(r.perm, r.local, u32(__double2loint(r.frac[0])),
+                    u32(__double2hiint(r.frac[0])));
+  d[1] = make_uint4(u32(__double2loint(r.frac[1])), u32(__double2hiint(r.frac[1])),
+                    u32(__double2loint(r.frac[2])), u32(__double2hiint(r.frac[2])));
+}
+// The whole sector of a record, as two 16-byte vectors (copies keep the sector whole).
+template <typename T>
+struct RecSector {
+  uint4 a, b;
+};
+template <typename T>
+__device__ __forceinline__ RecSector<T> load_sector(const PointRec<T>* src) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  return RecSector<T>{s[0], s[1]};
+}
+template <typename T>
+__device__ __forceinline__ void store_sector(PointRec<T>* dst, const RecSector<T>& v) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  d[0] = v.a;
+  d[1] = v.b;
+}
+
 // Device scratch of a point set for the kernels' work lists (worklist.cu).
 struct WorkScratch {
   u32* cnt;       // items per unit (max_units)
