@@ -21,22 +21,39 @@ constexpr int kBinBlock = 256;
 
 // First kernel cell of one coordinate: i0 = ceil(loc - w/2) wrapped to [0, nf), and the
 // kernel argument frac = i0 - loc in [-w/2, -w/2 + 1]. Returns false for non-finite input.
-__device__ __forceinline__ bool cell_of(const BinGeom& g, int d, double x, i64& i0w,
+// The wrap runs on the integral double (exact below 2^53), and the cell index, below nf <= 2^31
+// - 1 (make_geom), converts to a 32-bit int: no 64-bit integer arithmetic per point.
+__device__ __forceinline__ bool cell_of(const BinGeom& g, int d, double x, int& i0w,
                                         double& frac) {
   const double v = (x - g.offset[d]) * g.scale[d];
   double p = (v + kPi) * kTwoPiInv;
   p = p - floor(p);
   const double nf = double(g.nf[d]);
   const double loc = p * nf;
-  const double s = ceil(loc - 0.5 * double(g.w));
+  double s = ceil(loc - 0.5 * double(g.w));
   frac = s - loc;
   if (!(frac == frac) || !(fabs(frac) <= 16.0)) return false;
-  i64 i0 = static_cast<i64>(s);
-  const i64 n = g.nf[d];
-  while (i0 < 0) i0 += n;
-  while (i0 >= n) i0 -= n;
-  i0w = i0;
+  while (s < 0.0) s += nf;
+  while (s >= nf) s -= nf;
+  i0w = __double2int_rz(s);
   return true;
+}
+
+// Quotient and remainder of a cell index by a tile extent (inv_t = 1 / t), from a double
+// product and one correction step: for an index under 2^31 the product is off the true quotient
+// by far less than one, so the truncated quotient is off by at most one either way. A 64-bit
+// integer division here is a long instruction sequence, three per point, and made the binning
+// scatter issue-bound.
+__device__ __forceinline__ void tile_divmod(int i, int t, double inv_t, int& q, int& r) {
+  q = __double2int_rz(double(i) * inv_t);
+  r = int(i64(i) - i64(q) * t);
+  if (r < 0) {
+    --q;
+    r += t;
+  } else if (r >= t) {
+    ++q;
+    r -= t;
+  }
 }
 
 // Points per thread and loop trip: the kernels are bound by memory latency (the coordinate
@@ -61,6 +78,9 @@ template <typename T, int DIM>
 __global__ void __launch_bounds__(kBinBlock)
     bin_count_kernel(BinGeom g, CoordPtrs<T> x, i64 M, u32* counts, u32* ranks, int* err) {
   const i64 stride = i64(gridDim.x) * kBinBlock;
+  double inv_tile[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) inv_tile[d] = 1.0 / double(g.tile[d]);
   for (i64 base = blockIdx.x * i64(kBinBlock) + threadIdx.x; base < M;
        base += stride * kBinUnroll) {
     T v[kBinUnroll][DIM];
@@ -77,10 +97,11 @@ __global__ void __launch_bounds__(kBinBlock)
       bool ok = true;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
-        i64 i0 = 0;
+        int i0 = 0, q, rem;
         double frac;
         ok &= cell_of(g, d, double(v[u][d]), i0, frac);
-        t[d] = i0 / g.tile[d];
+        tile_divmod(i0, g.tile[d], inv_tile[d], q, rem);
+        t[d] = q;
       }
       tile_lin[u] = tile_linear_d<DIM>(g, t);
       if (!ok && base + u * stride < M) {
@@ -105,6 +126,9 @@ __global__ void __launch_bounds__(kBinBlock)
     bin_scatter_kernel(BinGeom g, CoordPtrs<T> x, i64 M, const u32* ranks, const u32* bin_start,
                        PointRec<T>* recs) {
   const i64 stride = i64(gridDim.x) * kBinBlock;
+  double inv_tile[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) inv_tile[d] = 1.0 / double(g.tile[d]);
   for (i64 base = blockIdx.x * i64(kBinBlock) + threadIdx.x; base < M;
        base += stride * kBinUnroll) {
     T v[kBinUnroll][DIM];
@@ -123,7 +147,7 @@ __global__ void __launch_bounds__(kBinBlock)
       i64 t[3] = {0, 0, 0};
       int l[3] = {0, 0, 0};
       double fr[3] = {0, 0, 0};
-      i64 i0[3] = {0, 0, 0};
+      int i0[3] = {0, 0, 0};
       bool ok = true;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) ok &= cell_of(g, d, double(v[u][d]), i0[d], fr[d]);
@@ -135,8 +159,9 @@ __global__ void __launch_bounds__(kBinBlock)
           i0[d] = 0;
           fr[d] = -0.5 * g.w;
         }
-        t[d] = i0[d] / g.tile[d];
-        l[d] = int(i0[d] - t[d] * g.tile[d]);
+        int q;
+        tile_divmod(i0[d], g.tile[d], inv_tile[d], q, l[d]);
+        t[d] = q;
       }
       tile_lin[u] = tile_linear_d<DIM>(g, t);
       r[u].perm = u32(base + u * stride);

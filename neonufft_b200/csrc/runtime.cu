@@ -357,6 +357,8 @@ BinGeom make_geom(int dim, int w, const i64* nf, const int* tile, const double* 
   g.total_tiles = 1;
   for (int d = 0; d < 3; ++d) {
     if (d < dim) {
+      // the binning kernels hold cell indices in 32-bit ints (cuFFT's own limit as well)
+      if (nf[d] > i64(0x7fffffff)) throw_input("fine grid dimension too large");
       g.nf[d] = nf[d];
       g.tile[d] = tile[d];
       g.ntiles[d] = int((nf[d] + tile[d] - 1) / tile[d]);
