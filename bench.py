@@ -1,17 +1,27 @@
 #!/usr/bin/env python
 """Benchmark of the B200 NUFFT engine (one JSON line on rank 0).
 
-Workload (default ``c2``): 3D type-2 + type-1 round pair, M = 1e7 points i.i.d. uniform in
-[-pi, pi)^3 (float32), N = 128^3 complex64 modes N(0,1), complex64 strengths N(0,1), tol 1e-6,
-upsampfac 2 (fine grid 256^3). Synthetic, seeded data; no public dataset is involved.
+Workload (default ``ns``): 3D type 1, M = 1e8 points i.i.d. uniform in [-pi, pi)^3, complex64
+strengths N(0,1), N = 256^3 modes, tol 1e-6, upsampfac 2 (fine grid 512^3). Synthetic, seeded
+data; no public dataset is involved. One step = set_points (binning) + transform_type_1, so the
+metric, NU points per second per transform, is M / step time (set_points included).
 
-One step = set_points (binning) + transform_type_2 + transform_type_1 on the same points, so
-the metric, NU points per second per transform, is 2 M / step time (set_points included).
-``--workload ns`` runs the 3D type-1 case M = 1e8, N = 256^3 (step = set_points + type 1).
+Arms of the same run, on the same points and strengths:
+  - the tuned single-precision engine (width 8, 4-row z-window tiles): ``value`` and ``e2e``;
+  - ``plain_fp64``: the engine's plain FP64 path (reference heuristic w = 7, default tiles),
+    the denominator of ``ratio_vs_plain_fp64``;
+  - ``reference_gpu_fp64``: the reference's own FP64 GPU plan, compiled from its sources for
+    sm_100a (oracle/_ref), when that build is present.
+Every arm's accuracy is the relative l2 error against FP64 direct sums on 1e4 sampled outputs;
+the run exits nonzero when the tuned arm misses tol.
+
+``--workload c2`` runs the 3D type-2 + type-1 round pair (M = 1e7, N = 128^3; step = set_points
++ type 2 + type 1); ``c1`` the 2D type-1 case; ``c3``, ``c4``, ``c5`` the type-3, batched and
+tuner workloads.
 
 Timing: W untimed warm-up steps, then K steps between CUDA events on the plan's stream,
-bracketed by barrier + synchronize, max over ranks. The inputs (coordinates 120 MB, strengths
-80 MB, modes 17 MB, fine grid 134 MB) exceed the 126 MB L2, so no extra flush is done.
+bracketed by barrier + synchronize, max over ranks. The inputs (north star: coordinates 1.2 GB,
+strengths 0.8 GB, fine grid 1 GiB) exceed the 126 MB L2, so no extra flush is done.
 
 Multi-GPU: the path does not shard a single transform; ranks run independent replicas
 (weak scaling, no data-path collective) and ``value`` sums the points of all ranks.
@@ -62,16 +72,6 @@ WORKLOADS = {
                dim=2, M=100_000, N=256, tol=1e-6, types=(1,), seed=1, cpu_sample=100_000,
                tuned_w=8),
 }
-# DRAM bytes (read + write) per point of one launch of the dominant kernel, from one ncu capture
-# of the same configuration (profiles/zwin_c2.md): (workload, precision, method, n_spread, tile,
-# kernel) -> bytes per point.
-DRAM_BYTES_PER_POINT = {
-    ("c2", "f32", 3, 8, (4, 8, 1), "interp"): (669.191936e6 + 261.929472e6) / 1e7,
-    ("c2", "f32", 3, 8, (4, 8, 1), "spread"): (959.445760e6 + 144.172288e6) / 1e7,
-    ("c2", "f32", 3, 8, (8, 8, 1), "interp"): (665.430528e6 + 261.607424e6) / 1e7,
-    ("c2", "f32", 3, 8, (8, 8, 1), "spread"): (943.662592e6 + 131.524864e6) / 1e7,
-}
-
 METRIC = "NU points/sec per transform at rel-l2 <=1e-6 (tuned FP32 vs plain GPU; CPU ref)"
 UNIT = "points/s"
 
@@ -603,43 +603,168 @@ def run_type3(args, wl):
     return 0
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--samples", type=int, default=10000)
-    ap.add_argument("--spread-method", type=int, default=0,
-                    help="engine spreading/interpolation method (0 = plan default)")
-    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
-                    help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
-    ap.add_argument("--streams", type=int, default=8, help="internal streams of a batch (c4)")
-    ap.add_argument("--upsampfac", type=float, default=2.0, help="upsampling factor sigma")
-    ap.add_argument("--tile", default="",
-                    help="engine tile shape, e.g. 4,8,1 (default: the workload's tuned tile, "
-                         "else the plan's choice)")
-    ap.add_argument("--n-spread", type=int, default=-1,
-                    help="kernel width (0 = reference heuristic; default: the tuned width)")
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-    wl = WORKLOADS[args.workload]
-    if args.impl == "reference":
-        if "batch" in wl or "tuner" in wl or "t3" in wl:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              "this workload has no CPU reference arm"}))
-            return 0
-        return run_reference(args, wl)
-    if "batch" in wl:
-        return run_batch(args, wl)
-    if "tuner" in wl:
-        return run_tuner(args, wl)
-    if "t3" in wl:
-        return run_type3(args, wl)
+def load_traffic(workload, precision, kernel, w, tile):
+    """DRAM bytes (read + write) of one launch of `kernel`, as a linear model a*M + b fitted to
+    ncu captures of the same configuration, from the committed summary profiles/dram_traffic.md
+    (rows '| workload | precision | kernel | w | tile | a | b |'). None when not captured."""
+    p = ROOT / "profiles" / "dram_traffic.md"
+    if not p.exists():
+        return None
+    key = (workload, precision, kernel, str(w), ",".join(str(int(v)) for v in tile))
+    for line in p.read_text().splitlines():
+        cells = [x.strip() for x in line.strip().strip("|").split("|")]
+        if len(cells) >= 7 and tuple(cells[:5]) == key:
+            try:
+                return float(cells[5]), float(cells[6])
+            except ValueError:
+                return None
+    return None
 
+
+def sampled_direct_sums(nnb, torch, wl, loc, c, f, S):
+    """FP64 direct sums (csrc/direct.cu, pinned against the CPU oracle by the GPU tests) on S
+    sampled outputs: type 1 at S random modes, type 2 at S random points."""
+    dim, M, N = wl["dim"], wl["M"], wl["N"]
+    nm = N ** dim
+    gs = torch.Generator(device="cuda")
+    gs.manual_seed(123)
+    loc64 = [a.double() for a in loc]
+    refs = {}
+    if 1 in wl["types"]:
+        idx = torch.randint(0, nm, (S,), generator=gs, device="cuda")
+        kk, rem = [], idx.clone()
+        for _ in range(dim):
+            kk.append(rem % N - N // 2)
+            rem = rem // N
+        kidx = torch.stack(kk, dim=1).contiguous()
+        ref = torch.empty(S, dtype=torch.complex128, device="cuda")
+        nnb.direct_type1_f64(-1, loc64, c.to(torch.complex128), kidx, ref)
+        refs[1] = (idx, ref)
+    if 2 in wl["types"]:
+        pidx = torch.randint(0, M, (S,), generator=gs, device="cuda")
+        ref = torch.empty(S, dtype=torch.complex128, device="cuda")
+        nnb.direct_type2_f64(-1, [N] * dim, f.to(torch.complex128), loc64, pidx, ref)
+        refs[2] = (pidx, ref)
+    torch.cuda.synchronize()
+    return refs
+
+
+def arm_accuracy(torch, refs, outs):
+    """Relative l2 error of each type's sampled outputs against the direct sums."""
+    acc = {}
+    for t, (idx, ref) in refs.items():
+        got = outs[t][idx].to(torch.complex128)
+        acc[f"type{t}_rel_l2"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+    return acc
+
+
+def timed_steps(torch, step, steps, warmup, barrier):
+    """Device time per step (CUDA events on the current stream), max over ranks."""
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+
+def plain_fp64_arm(nnb, torch, wl, args, loc, c, f, refs, barrier):
+    """The plain single-transform FP64 GPU path of the engine: double precision, the reference's
+    parameter heuristic (w = 7 at tol 1e-6, upsampfac 2), default method and tiles, no batching,
+    no graphs, no tuner -- the denominator of the tuned engine's speed-up. Same points and
+    strengths (promoted exactly), same step, same number of timed steps."""
+    dim, M, N = wl["dim"], wl["M"], wl["N"]
+    nm = N ** dim
+    strides = [1, N, N * N][:dim]
+    lc = [a.double() for a in loc]
+    cc = c.to(torch.complex128)
+    ff = f.to(torch.complex128) if f is not None else None
+    o1 = torch.empty(nm, dtype=torch.complex128, device="cuda") if 1 in wl["types"] else None
+    o2 = torch.empty(M, dtype=torch.complex128, device="cuda") if 2 in wl["types"] else None
+    plan = nnb.Plan(nnb.Options(tol=wl["tol"], upsampfac=2.0), -1, M, lc, [N] * dim)
+    info = plan.info()
+
+    def step():
+        plan.set_points(M, lc)
+        for t in wl["types"]:
+            if t == 2:
+                plan.transform_type_2(ff, strides, o2)
+            else:
+                plan.transform_type_1(cc, o1, strides)
+
+    plan.enable_timing(True)
+    ms = timed_steps(torch, step, args.steps, args.warmup, barrier)
+    stages = plan.stage_times(reset=True)
+    acc = arm_accuracy(torch, refs, {1: o1, 2: o2}) if refs else {}
+    plan.close()
+    del lc, cc, ff, o1, o2
+    torch.cuda.empty_cache()
+    ntr = len(wl["types"])
+    return {"ms_per_step": ms, "points_per_s": ntr * M / (ms * 1e-3), "steps": args.steps,
+            "precision": "f64", "n_spread": info["n_spread"], "method": info["spread_method"],
+            "tile": info["tile"][:dim], "accuracy": acc,
+            "stages_ms_per_step": {k: v[0] / (args.steps + args.warmup) for k, v in stages.items()
+                                   if v[1]}}
+
+
+def reference_gpu_arm(torch, wl, args, loc, c, f, refs, barrier):
+    """The reference's own FP64 GPU plan (its src/neonufft/gpu/plan_impl.hpp:91-113 path, compiled
+    from its sources for sm_100a into oracle/_ref) on the same points and strengths, same step,
+    on the legacy default stream where it launches. A measured baseline, never the product."""
+    try:
+        from oracle import oracle as O
+        L = O.Ref().L
+    except Exception as exc:  # the reference build is a checker, absent on some boxes
+        return {"unavailable": f"reference GPU build (oracle/_ref) not loadable: {exc}"}
+    if torch.cuda.current_stream().cuda_stream != 0:
+        return {"unavailable": "the reference plan launches on the legacy default stream"}
+    import ctypes as C
+    dim, M, N = wl["dim"], wl["M"], wl["N"]
+    nm = N ** dim
+    lc = [a.double() for a in loc]
+    cc = c.to(torch.complex128)
+    ff = f.to(torch.complex128) if f is not None else None
+    o1 = torch.empty(nm, dtype=torch.complex128, device="cuda") if 1 in wl["types"] else None
+    o2 = torch.empty(M, dtype=torch.complex128, device="cuda") if 2 in wl["types"] else None
+    lp = (C.c_void_p * 3)(*([a.data_ptr() for a in lc] + [0] * (3 - dim)))
+    md = (C.c_int64 * 3)(*([N] * dim + [1] * (3 - dim)))
+    st = (C.c_int64 * 3)(*([1, N, N * N][:dim] + [1] * (3 - dim)))
+    h = C.c_void_p()
+    rc = L.ref_plan12_create(C.byref(h), 0, dim, wl["tol"], 2.0, -1, M, lp, md)
+    if rc != 0:
+        return {"unavailable": f"reference plan creation failed with code {rc}"}
+
+    def step():
+        assert L.ref_plan12_set_points(h, M, lp) == 0
+        for t in wl["types"]:
+            if t == 2:
+                assert L.ref_plan12_t2(h, ff.data_ptr(), st, o2.data_ptr()) == 0
+            else:
+                assert L.ref_plan12_t1(h, cc.data_ptr(), o1.data_ptr(), st) == 0
+
+    steps = max(1, min(args.steps, args.ref_steps))
+    ms = timed_steps(torch, step, steps, 1, barrier)
+    acc = arm_accuracy(torch, refs, {1: o1, 2: o2}) if refs else {}
+    L.ref_plan12_destroy(h)
+    torch.cuda.synchronize()
+    del lc, cc, ff, o1, o2
+    torch.cuda.empty_cache()
+    ntr = len(wl["types"])
+    return {"ms_per_step": ms, "points_per_s": ntr * M / (ms * 1e-3), "steps": steps,
+            "warmup": 1, "precision": "f64", "accuracy": acc,
+            "source": "reference GPU plan built from its own sources (oracle/_ref)"}
+
+
+def run_transform(args, wl):
+    """Single-transform workloads (ns, c2, c1): the tuned engine arm (the line's value and e2e),
+    then the plain FP64 arm and the reference's FP64 GPU plan on the same inputs."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -657,21 +782,29 @@ def main():
             dist.barrier()
 
     dim, M, N, tol = wl["dim"], wl["M"], wl["N"], wl["tol"]
+    types = wl["types"]
     g = torch.Generator(device="cuda")
     g.manual_seed(rank_seed(wl, rank))
+    # Points and strengths are drawn in single precision and promoted exactly for the double
+    # precision arms and the FP64 direct sums, so that every arm sees the same inputs.
+    loc = [(torch.rand(M, generator=g, device="cuda", dtype=torch.float32) * 2 - 1) * math.pi
+           for _ in range(dim)]
+    c = torch.complex(torch.randn(M, generator=g, device="cuda", dtype=torch.float32),
+                      torch.randn(M, generator=g, device="cuda", dtype=torch.float32))
+    nm = N ** dim
+    f = (torch.complex(torch.randn(nm, generator=g, device="cuda", dtype=torch.float32),
+                       torch.randn(nm, generator=g, device="cuda", dtype=torch.float32))
+         if 2 in types else None)
     f64 = args.precision == "f64"
     rdt = torch.float64 if f64 else torch.float32
     cdt = torch.complex128 if f64 else torch.complex64
     rsz = 8 if f64 else 4  # bytes per real
-    loc = [(torch.rand(M, generator=g, device="cuda", dtype=rdt) * 2 - 1) * math.pi
-           for _ in range(dim)]
-    c = torch.complex(torch.randn(M, generator=g, device="cuda", dtype=rdt),
-                      torch.randn(M, generator=g, device="cuda", dtype=rdt))
-    nm = N ** dim
-    f = torch.complex(torch.randn(nm, generator=g, device="cuda", dtype=rdt),
-                      torch.randn(nm, generator=g, device="cuda", dtype=rdt))
-    out1 = torch.empty(nm, dtype=cdt, device="cuda")
-    out2 = torch.empty(M, dtype=cdt, device="cuda")
+    if f64:
+        loc = [a.double() for a in loc]
+        c = c.to(cdt)
+        f = f.to(cdt) if f is not None else None
+    out1 = torch.empty(nm, dtype=cdt, device="cuda") if 1 in types else None
+    out2 = torch.empty(M, dtype=cdt, device="cuda") if 2 in types else None
     strides = [1, N, N * N][:dim]
     modes = [N] * dim
     # The reference heuristic gives w = 7 at tol 1e-6, whose truncation error alone is ~1.5e-6
@@ -689,7 +822,7 @@ def main():
 
     def step(lc, ff, cc, o2, o1):
         plan.set_points(M, lc)
-        for t in wl["types"]:
+        for t in types:
             if t == 2:
                 plan.transform_type_2(ff, strides, o2)
             else:
@@ -721,7 +854,7 @@ def main():
     plan.enable_timing(False)
     ms = max_over_ranks(e0.elapsed_time(e1))
     ms_step = ms / args.steps
-    ntr = len(wl["types"])
+    ntr = len(types)
     value = job_throughput(world, ntr * M, ms_step)
 
     # ---- end-to-end through the public API with host buffers --------------------------------
@@ -729,16 +862,18 @@ def main():
     loc_h = [torch.empty(M, dtype=rdt, **pin) for _ in range(dim)]
     for a, b in zip(loc_h, loc):
         a.copy_(b)
-    c_h = torch.empty(M, dtype=cdt, **pin)
-    c_h.copy_(c)
-    f_h = torch.empty(nm, dtype=cdt, **pin)
-    f_h.copy_(f)
-    o1_h = torch.empty(nm, dtype=cdt, **pin)
-    o2_h = torch.empty(M, dtype=cdt, **pin)
+    c_h = f_h = o1_h = o2_h = None
+    if 1 in types:
+        c_h = torch.empty(M, dtype=cdt, **pin)
+        c_h.copy_(c)
+        o1_h = torch.empty(nm, dtype=cdt, **pin)
+    if 2 in types:
+        f_h = torch.empty(nm, dtype=cdt, **pin)
+        f_h.copy_(f)
+        o2_h = torch.empty(M, dtype=cdt, **pin)
     csz = 2 * rsz
-    h2d = (dim * M * rsz + (M * csz if 1 in wl["types"] else 0)
-           + (nm * csz if 2 in wl["types"] else 0))
-    d2h = (nm * csz if 1 in wl["types"] else 0) + (M * csz if 2 in wl["types"] else 0)
+    h2d = dim * M * rsz + (M * csz if 1 in types else 0) + (nm * csz if 2 in types else 0)
+    d2h = (nm * csz if 1 in types else 0) + (M * csz if 2 in types else 0)
 
     # Pipelined as a caller would run a stream of transforms: two device buffer sets; step i's
     # host->device copies run on an upload stream while step i-1 computes, and step i-1's
@@ -746,9 +881,11 @@ def main():
     # of a buffer set; every step still moves all of its inputs and outputs.
     comp = torch.cuda.current_stream()
     up, down = torch.cuda.Stream(), torch.cuda.Stream()
-    bufs = [{"loc": [torch.empty_like(a) for a in loc], "c": torch.empty_like(c),
-             "f": torch.empty_like(f), "o1": torch.empty_like(out1), "o2": torch.empty_like(out2)}
-            for _ in range(2)]
+
+    def like(x):
+        return torch.empty_like(x) if x is not None else None
+    bufs = [{"loc": [torch.empty_like(a) for a in loc], "c": like(c), "f": like(f),
+             "o1": like(out1), "o2": like(out2)} for _ in range(2)]
     uploaded = [torch.cuda.Event() for _ in range(2)]
     computed = [torch.cuda.Event() for _ in range(2)]
     downloaded = [torch.cuda.Event() for _ in range(2)]
@@ -762,9 +899,9 @@ def main():
         with torch.cuda.stream(up):
             for a, h in zip(b["loc"], loc_h):
                 a.copy_(h, non_blocking=True)
-            if 1 in wl["types"]:
+            if 1 in types:
                 b["c"].copy_(c_h, non_blocking=True)
-            if 2 in wl["types"]:
+            if 2 in types:
                 b["f"].copy_(f_h, non_blocking=True)
         uploaded[j].record(up)
         comp.wait_event(uploaded[j])
@@ -773,9 +910,9 @@ def main():
         computed[j].record(comp)
         down.wait_event(computed[j])
         with torch.cuda.stream(down):
-            if 1 in wl["types"]:
+            if 1 in types:
                 o1_h.copy_(b["o1"], non_blocking=True)
-            if 2 in wl["types"]:
+            if 2 in types:
                 o2_h.copy_(b["o2"], non_blocking=True)
         downloaded[j].record(down)
 
@@ -793,64 +930,59 @@ def main():
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = job_throughput(world, ntr * M, ms_e2e / args.steps)
+    plan.close()
+    del bufs, loc_h, c_h, f_h, o1_h, o2_h
+    torch.cuda.empty_cache()
 
     # ---- accuracy vs the FP64 direct sum on sampled outputs (not timed) ---------------------
+    refs = None
     acc = {}
     if not args.no_accuracy:
         S = min(args.samples, 65535)
-        gs = torch.Generator(device="cuda")
-        gs.manual_seed(123)
-        loc64 = [a.double() for a in loc]
-        if 1 in wl["types"]:
-            idx = torch.randint(0, nm, (S,), generator=gs, device="cuda")
-            kk = []
-            rem = idx.clone()
-            for d in range(dim):
-                kk.append(rem % N - N // 2)
-                rem = rem // N
-            kidx = torch.stack(kk, dim=1).contiguous()
-            ref = torch.empty(S, dtype=torch.complex128, device="cuda")
-            nnb.direct_type1_f64(-1, loc64, c.to(torch.complex128), kidx, ref)
-            got = out1[idx].to(torch.complex128)
-            acc["type1_rel_l2"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
-        if 2 in wl["types"]:
-            pidx = torch.randint(0, M, (S,), generator=gs, device="cuda")
-            ref = torch.empty(S, dtype=torch.complex128, device="cuda")
-            nnb.direct_type2_f64(-1, modes, f.to(torch.complex128), loc64, pidx, ref)
-            got = out2[pidx].to(torch.complex128)
-            acc["type2_rel_l2"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        refs = sampled_direct_sums(nnb, torch, wl, loc, c, f, S)
+        acc = arm_accuracy(torch, refs, {1: out1, 2: out2})
         acc["samples"] = S
-        torch.cuda.synchronize()
+        acc["tol"] = tol
+        acc["meets_tol"] = all(v <= tol for k, v in acc.items() if k.endswith("rel_l2"))
+
+    # ---- the plain FP64 GPU path and the reference's FP64 GPU plan (same inputs) ------------
+    plain = ref_gpu = None
+    if not args.no_extra_arms:
+        plain = plain_fp64_arm(nnb, torch, wl, args, loc, c, f, refs, barrier)
+        ref_gpu = reference_gpu_arm(torch, wl, args, loc, c, f, refs, barrier)
 
     # ---- roofline of the dominant kernel -----------------------------------------------------
     peak, peak_kind = load_peaks()
-    spread_ms = stages["spread"][0] / max(1, stages["spread"][1])
+    spread_ms = stages["spread"][0] / max(1, stages["spread"][1]) if stages["spread"][1] else 0.0
     interp_ms = stages["interp"][0] / max(1, stages["interp"][1]) if stages["interp"][1] else 0.0
     w = info["n_spread"]
     nf_cells = int(np.prod(info["grid"][:dim]))
-    # Algorithmic bytes of one launch: per point its 32-byte bin-sorted record and its complex
-    # strength (spreading) or output (interpolation), plus one pass over the complex fine grid.
-    csz = 16 if f64 else 8
-    spread_bytes = M * (32 + csz) + nf_cells * csz
-    spread_flop = M * 5 * w ** dim
-    dom = "spread"
-    dom_ms, dom_bytes, dom_flop = spread_ms, spread_bytes, spread_flop
-    if interp_ms > spread_ms:
-        dom = "interp"
-        dom_ms = interp_ms
-        dom_bytes = M * (32 + csz) + nf_cells * csz
-        dom_flop = M * 5 * w ** dim
-    key = (args.workload, args.precision, info["spread_method"], w, tuple(info["tile"][:dim]), dom)
-    traffic = (DRAM_BYTES_PER_POINT[key] * M) if key in DRAM_BYTES_PER_POINT else None
-    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    # Algorithmic bytes of one spreading (or interpolation) launch: per point its d coordinates
+    # and its complex strength (or output), d + 2 reals, plus one complex fine-grid pass:
+    # M (d + 2) s_T + 2 s_T nf^d.
+    alg_bytes = M * (dim + 2) * rsz + 2 * rsz * nf_cells
+    alg_flop = M * 5 * w ** dim
+    dom, dom_ms, kname = ("interp", interp_ms, "interp_zwin_kernel") if interp_ms > spread_ms \
+        else ("spread", spread_ms, "spread_zwin_kernel")
+    if info["spread_method"] != 3:
+        kname = {"spread": "spread_slab_kernel", "interp": "interp_slab_kernel"}[dom]
+    model = load_traffic(args.workload, args.precision, kname, w, info["tile"][:dim])
+    traffic = (model[0] * M + model[1]) if model else None
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
     roofline = {
-        "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} HBM copy",
-        "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
-        "fp32": {"achieved_tflops": dom_flop / (dom_ms * 1e-3) / 1e12,
+        "bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": traffic,
+        "peak_source": f"{peak_kind} HBM copy (MEASURED_PEAKS.json hbm_gbs)",
+        "algorithmic_bytes_per_launch": alg_bytes,
+        "algorithmic_bytes_formula": "M (d + 2) s_T + 2 s_T nf^d",
+        "launch_ms": dom_ms,
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, linear fit a M + b "
+                           "from profiles/dram_traffic.md" if model else
+                           "not captured for this configuration"),
+        "fp32": {"achieved_tflops": alg_flop / (dom_ms * 1e-3) / 1e12,
                  "peak_tflops_nominal": fp32_peak,
-                 "frac": dom_flop / (dom_ms * 1e-3) / 1e12 / fp32_peak,
+                 "frac": alg_flop / (dom_ms * 1e-3) / 1e12 / fp32_peak,
                  "flop_per_point": 5 * w ** dim},
     }
 
@@ -875,10 +1007,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic (seeded uniform points, N(0,1) strengths and modes)",
-            "config": {"workload": wl["name"], "M": M, "N": N, "dim": dim, "tol": tol,
+            "config": {"workload": wl["name"], "workload_id": args.workload, "M": M, "N": N,
+                       "dim": dim, "tol": tol, "types": list(types),
                        "upsampfac": args.upsampfac, "n_spread": w, "fine_grid": info["grid"][:dim],
                        "tile": info["tile"][:dim], "method": info["spread_method"],
                        "precision": args.precision,
+                       "step": "set_points + " + " + ".join(f"transform_type_{t}" for t in types),
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (126 MB); no flush"},
             "clocks": clk,
@@ -893,12 +1027,69 @@ def main():
             "cpu_baseline": cpu,
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
             "accuracy": acc,
+            "plain_fp64": plain,
+            "ratio_vs_plain_fp64": (value / plain["points_per_s"]) if plain else None,
+            "reference_gpu_fp64": ref_gpu,
+            "ratio_vs_reference_gpu_fp64": (value / ref_gpu["points_per_s"])
+            if ref_gpu and "points_per_s" in ref_gpu else None,
         }
         print(json.dumps(line), flush=True)
-    plan.close()
     if world > 1:
         dist.destroy_process_group()
+    if acc and not acc["meets_tol"]:
+        print(f"bench: accuracy {acc} exceeds tol {tol}", file=sys.stderr, flush=True)
+        return 1
     return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="ns", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--samples", type=int, default=10000)
+    ap.add_argument("--no-extra-arms", action="store_true",
+                    help="skip the plain FP64 arm and the reference GPU plan arm")
+    ap.add_argument("--points", type=int, default=0,
+                    help="override the workload's point count M (small ncu captures of the same "
+                         "grid); the line records the M it ran")
+    ap.add_argument("--ref-steps", type=int, default=3,
+                    help="timed steps of the reference GPU plan arm (at most --steps)")
+    ap.add_argument("--spread-method", type=int, default=0,
+                    help="engine spreading/interpolation method (0 = plan default)")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                    help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
+    ap.add_argument("--streams", type=int, default=8, help="internal streams of a batch (c4)")
+    ap.add_argument("--upsampfac", type=float, default=2.0, help="upsampling factor sigma")
+    ap.add_argument("--tile", default="",
+                    help="engine tile shape, e.g. 4,8,1 (default: the workload's tuned tile, "
+                         "else the plan's choice)")
+    ap.add_argument("--n-spread", type=int, default=-1,
+                    help="kernel width (0 = reference heuristic; default: the tuned width)")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    wl = dict(WORKLOADS[args.workload])
+    if args.points > 0 and "M" in wl:
+        wl["M"] = args.points
+        wl["cpu_sample"] = min(wl.get("cpu_sample", args.points), args.points)
+    if args.impl == "reference":
+        if "batch" in wl or "tuner" in wl or "t3" in wl:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "this workload has no CPU reference arm"}))
+            return 0
+        return run_reference(args, wl)
+    if "batch" in wl:
+        return run_batch(args, wl)
+    if "tuner" in wl:
+        return run_tuner(args, wl)
+    if "t3" in wl:
+        return run_type3(args, wl)
+
+    return run_transform(args, wl)
 
 
 if __name__ == "__main__":

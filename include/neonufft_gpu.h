@@ -247,7 +247,9 @@ NNB_API NeonufftError nnb_direct_type3_f64(int dim, int sign, int64_t num_in, co
  * added in a fixed order, so the result is also bit-reproducible. Limit:
  * num_samples * ceil(num_nu / 4096) <= 1048576, else NEONUFFT_INPUT_ERROR. Nothing is
  * allocated; the first call on a device looks up the scratch address (make it before any
- * stream capture). All calls share the scratch: calls that overlap on the GPU race. */
+ * stream capture) and keeps it for the life of the process, so do not call this entry point
+ * after cudaDeviceReset (or any other destruction of the device's primary context) in the same
+ * process. All calls share the scratch: calls that overlap on the GPU race. */
 NNB_API NeonufftError nnb_direct_type1_f64_noalloc(int dim, int sign, int64_t num_nu,
                                                    const double* const* loc, const double* in,
                                                    int64_t num_samples,

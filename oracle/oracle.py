@@ -37,11 +37,15 @@ _lib = None
 
 
 def build() -> None:
-    """Builds libnufft_oracle.so (and the reference pin library when the reference exists)."""
+    """Builds libnufft_oracle.so, and the reference pin library when NEONUFFT_REFERENCE_DIR names
+    a NeoNUFFT source checkout."""
+    import os
     import subprocess
     subprocess.run(["make", "-C", str(HERE), "all"], check=True, capture_output=True)
-    if Path("/root/reference").exists():
-        subprocess.run(["make", "-C", str(HERE), "ref", "-j8"], check=True, capture_output=True)
+    ref = os.environ.get("NEONUFFT_REFERENCE_DIR", "")
+    if ref and Path(ref).is_dir():
+        subprocess.run(["make", "-C", str(HERE), "ref", f"REF={ref}", "-j8"], check=True,
+                       capture_output=True)
 
 
 def lib() -> C.CDLL:

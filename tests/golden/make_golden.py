@@ -1,7 +1,7 @@
 """Generates the committed golden fixtures of tests/golden/ from the reference's own code.
 
-Run in the development container (needs /root/reference and `make -C oracle ref`):
-    python tests/golden/make_golden.py
+Run where the reference's sources are present (after `make -C oracle ref REF=<checkout>`):
+    NEONUFFT_REFERENCE_DIR=<checkout> python tests/golden/make_golden.py
 
 Writes
   pins.json  -- values computed by the reference's own host code compiled from its sources

@@ -157,3 +157,37 @@ def test_t3_invalid_bounds(engine):
     size = C.c_uint64()
     assert lib.nnb_plan_t3_grid_memory_size(0, 1, None, None, None, None, None,
                                             C.byref(size)) == _lib.INPUT_ERROR
+
+
+def test_noalloc_rejects_requests_beyond_its_scratch():
+    """The allocation-free direct sum rejects sizes beyond its fixed scratch before any device
+    work. Run in a child process that sees no GPU (CUDA_VISIBLE_DEVICES empty), so that a
+    regressed size check ends in a CUDA error there rather than in a launch over these
+    placeholder buffers."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import ctypes as C
+from neonufft_b200 import _lib as L
+lib = L.load()
+M, S = 4096 * 20000, 60  # 60 samples x 20000 chunks > 2^20 partial sums
+buf = (C.c_double * 256)()
+ptrs = L.ptr_array([C.addressof(buf)])
+kidx = (C.c_int64 * (S + 1))()
+rc = lib.nnb_direct_type1_f64_noalloc(1, -1, M, ptrs, C.addressof(buf), S, C.addressof(kidx),
+                                      C.addressof(buf), None)
+msg = lib.nnb_last_error_message()
+assert rc == L.INPUT_ERROR, (rc, msg)
+assert b"scratch" in msg, msg
+# the largest request that fits is accepted by the size check (it then needs a device)
+M = 4096 * (1048576 // S)
+rc = lib.nnb_direct_type1_f64_noalloc(1, -1, M, ptrs, C.addressof(buf), S, C.addressof(kidx),
+                                      C.addressof(buf), None)
+assert rc != L.INPUT_ERROR or b"scratch" not in lib.nnb_last_error_message()
+print("ok")
+'''
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    res = subprocess.run([sys.executable, "-c", code], cwd=str(ROOT), env=env,
+                         capture_output=True, text=True, timeout=120)
+    assert res.returncode == 0 and "ok" in res.stdout, res.stdout + res.stderr
