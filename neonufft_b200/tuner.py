@@ -246,3 +246,58 @@ class Tuner:
             if r is not None and r[1] <= p.tol:
                 return cands[int(i)], r, tried
         return HEURISTIC, measure(p, HEURISTIC, data), len(cands)
+
+
+def rule_plus_one(p: Problem) -> Config:
+    """The simplest fix of the heuristic's tolerance misses: its width plus one, upsampfac 2,
+    the plan's default method and tile."""
+    return Config(2.0, min(16, heuristic_width(p.tol, 2.0, p.precision) + 1), 0, (0, 0, 0))
+
+
+def evaluate(tuner: Tuner, held, exhaustive: bool = True) -> dict:
+    """Scores the learned picks on held-out problems against the reference heuristic, the
+    width-plus-one rule and (optionally) exhaustive autotuning over every candidate.
+
+    Time ratios are geometric means of (other configuration's time / pick's time), each over
+    the problems where that configuration meets tol; `measurements_*` count the candidate
+    configurations measured (plan built, run, error checked) per problem."""
+    def geo(v):
+        return float(np.exp(np.mean(np.log(v)))) if v else None
+
+    r_heur, r_rule, r_best, tried, n_cands = [], [], [], [], []
+    heur_miss = rule_miss = pick_miss = 0
+    for p in held:
+        data = ProblemData(p)
+        cfg, (ms, err), k = tuner.pick(p, data)
+        tried.append(k)
+        pick_miss += int(err > p.tol)
+        h_ms, h_err = measure(p, HEURISTIC, data)
+        if h_err <= p.tol:
+            r_heur.append(h_ms / ms)
+        else:
+            heur_miss += 1
+        rr = measure_or_none(p, rule_plus_one(p), data)
+        if rr is not None and rr[1] <= p.tol:
+            r_rule.append(rr[0] / ms)
+        else:
+            rule_miss += 1
+        cands = candidates(p)
+        n_cands.append(len(cands))
+        if exhaustive:
+            best = None
+            for c in cands:
+                r = measure_or_none(p, c, data)
+                if r is not None and r[1] <= p.tol and (best is None or r[0] < best):
+                    best = r[0]
+            if best is not None:
+                r_best.append(best / ms)
+        del data
+    return {
+        "problems": len(held), "picks_missing_tol": pick_miss,
+        "heuristic_missed_tol": heur_miss, "rule_plus_one_missed_tol": rule_miss,
+        "speedup_vs_heuristic_geomean": geo(r_heur),
+        "speedup_vs_rule_plus_one_geomean": geo(r_rule),
+        "pick_time_over_exhaustive_best_geomean": (1.0 / geo(r_best)) if r_best else None,
+        "measurements_per_pick": float(np.mean(tried)) if tried else None,
+        "measurements_exhaustive": float(np.mean(n_cands)) if n_cands else None,
+    }

@@ -205,3 +205,52 @@ def test_batch_rejects_bad_requests(cuda, engine):
         engine.Batch(engine.Options(tol=1e-6), torch.float32, num_streams=0)
     batch.execute(engine.Batch.GRAPH)  # empty batch: nothing to do
     batch.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_batch_split_over_ranks(world, cuda, engine, oracle):
+    """One batch split over `world` ranks (neonufft_b200.replicas.ShardedBatch), the ranks
+    emulated one after another on this GPU (they never wait on one another): every transform
+    is held by exactly one rank, and the union of the ranks' outputs matches the FP64 direct
+    sums and the whole batch run by one process."""
+    from neonufft_b200 import replicas
+    torch = cuda
+    dtype, tol = "float32", 1e-5
+    rng = np.random.default_rng(43)
+    probs = make_problems(rng, dtype, 11)
+    costs = [replicas.transform_cost(p["dim"], p["M"], p["modes"], tol) for p in probs]
+    owners = replicas.shard_owners(costs, world)
+    outs = [None] * len(probs)
+    held = []
+    for rank in range(world):
+        sb = replicas.ShardedBatch(engine.Options(tol=tol), torch.float32, owners, rank,
+                                   num_streams=2)
+        for i, p in enumerate(probs):
+            if not sb.owns(i):
+                continue
+            loc, inp, out = device_buffers(torch, dtype, p)
+            sb.add(i, p["type"], p["sign"], loc, p["modes"], inp, out, col_strides(p["modes"]))
+            outs[i] = out
+        with pytest.raises(ValueError):
+            sb.add(next(i for i in range(len(probs)) if not sb.owns(i)), 1, -1, [], [8], None,
+                   None, [1])
+        sb.execute()
+        torch.cuda.synchronize()
+        held += sb.local
+        sb.close()
+    assert sorted(held) == list(range(len(probs)))
+    whole = engine.Batch(engine.Options(tol=tol), torch.float32, num_streams=2)
+    wouts = []
+    for p in probs:
+        loc, inp, out = device_buffers(torch, dtype, p)
+        whole.add(p["type"], p["sign"], loc, p["modes"], inp, out, col_strides(p["modes"]))
+        wouts.append(out)
+    whole.execute()
+    torch.cuda.synchronize()
+    for i, p in enumerate(probs):
+        got = outs[i].cpu().numpy()
+        ref = direct(oracle, p)
+        assert oracle.rel_l2(got, ref) <= 10 * tol
+        w = wouts[i].cpu().numpy()
+        assert np.linalg.norm(got - w) <= 1e-5 * np.linalg.norm(w)
+    whole.close()

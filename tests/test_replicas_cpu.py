@@ -61,3 +61,46 @@ def test_rank_failure_ends_the_job(tmp_path):
     r = _launch("raise", tmp_path, timeout=150)
     assert r.returncode != 0
     assert "rank 1 fails between steps" in (r.stdout + r.stderr)
+
+
+def test_shard_owners_balanced_and_deterministic():
+    from neonufft_b200 import replicas
+    costs = [5.0, 1.0, 4.0, 4.0, 3.0, 3.0, 2.0, 2.0, 9.0]
+    for world in (1, 2, 3, 4):
+        owners = replicas.shard_owners(costs, world)
+        assert owners == replicas.shard_owners(list(costs), world)
+        assert sorted(set(owners)) == list(range(min(world, len(costs))))
+        loads = replicas.shard_loads(costs, owners, world)
+        assert sum(loads) == pytest.approx(sum(costs))
+        # longest-processing-time bound: the largest load is at most 4/3 of the optimum,
+        # which is at least max(mean load, largest transform)
+        assert max(loads) <= 4.0 / 3.0 * max(sum(costs) / world, max(costs)) + 1e-9
+    with pytest.raises(ValueError):
+        replicas.shard_owners(costs, 0)
+
+
+def test_transform_cost_follows_work_and_grid():
+    from neonufft_b200 import replicas
+    a = replicas.transform_cost(3, 10 ** 6, [64] * 3)
+    assert replicas.transform_cost(3, 2 * 10 ** 6, [64] * 3) > a
+    assert replicas.transform_cost(3, 10 ** 6, [128] * 3) > a
+    # FP32 tol 1e-6: w = 7, fine grid 128^3
+    cells = 128.0 ** 3
+    import math
+    assert a == pytest.approx(1e6 * 7 ** 3 + 5 * cells * math.log2(cells))
+
+
+def test_one_batch_split_over_two_ranks(tmp_path):
+    """Each transform of the batch runs on exactly one rank, both ranks compute the same
+    assignment, and the union of the ranks' results equals one process running the whole
+    batch."""
+    r = _launch("shard", tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    recs = [json.loads((tmp_path / f"rank{i}.json").read_text()) for i in range(2)]
+    assert recs[0]["owners"] == recs[1]["owners"]
+    ran0, ran1 = set(recs[0]["ran"]), set(recs[1]["ran"])
+    assert not ran0 & ran1 and ran0 | ran1 == set(range(len(recs[0]["owners"])))
+    assert recs[0]["counts"] == [1] * len(recs[0]["owners"])
+    assert recs[0]["max_abs_diff"] == 0.0
+    loads = recs[0]["loads"]
+    assert max(loads) <= 4.0 / 3.0 * max(sum(loads) / 2, max(recs[0]["costs"]))
