@@ -340,6 +340,13 @@ NNB_API NeonufftError nnb_mlp_adam(int64_t n, float* params, const float* grads,
                                    int64_t step, void* stream);
 
 /* Library version string. */
+/* 1 for the bounds-checked debugging build (libneonufft_b200_checked.so, compiled with
+ * -DNNB_CHECKED: device bounds checks on the hot kernels' grid, record and output indices, and a
+ * device synchronisation after every call that reports a failed check as
+ * NEONUFFT_INTERNAL_ERROR), 0 for the normal build. Engine extension; the reference's
+ * counterpart is its debug-build sync-and-check after each launch
+ * (src/neonufft/gpu/util/runtime.hpp:27-30). */
+NNB_API int nnb_is_checked_build(void);
 NNB_API const char* nnb_version(void);
 
 /* Number of engine kernels this process has launched so far (all plans and devices; cuFFT's

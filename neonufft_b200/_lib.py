@@ -102,6 +102,7 @@ SIGNATURES = [
     ("nnb_mlp_adam", _E, [_I64, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P]),
     ("nnb_version", C.c_char_p, []),
     ("nnb_kernel_launches", C.c_int64, []),
+    ("nnb_is_checked_build", C.c_int, []),
 ]
 
 _lib = None

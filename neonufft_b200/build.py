@@ -5,7 +5,13 @@ Every CUDA source is compiled by nvcc with
 parallel), then linked with the CUDA runtime (static) and cuFFT (shared). Rebuilds only when a
 source, a header or this script is newer than the library.
 
-Usage: ``python -m neonufft_b200.build [--force] [--verbose]``.
+``--checked`` builds the checked variant libneonufft_b200_checked.so (objects in
+``_build_checked/``) with ``-DNNB_CHECKED``: device bounds checks on every grid, record and
+output index of the hot kernels, which record the first failure instead of accessing out of
+bounds, and a device synchronisation plus check after every C ABI call that reports a failure
+as InternalError (a debugging build; load it with NEONUFFT_B200_LIB).
+
+Usage: ``python -m neonufft_b200.build [--force] [--verbose] [--checked]``.
 """
 from __future__ import annotations
 
@@ -22,6 +28,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libneonufft_b200.so"
+BUILD_CHECKED = PKG / "_build_checked"
+LIB_CHECKED = PKG / "libneonufft_b200_checked.so"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -56,16 +64,17 @@ def _headers() -> list[Path]:
     return hs
 
 
-def _stale(extra: list[Path]) -> bool:
-    if not LIB.exists():
+def _stale(lib: Path, extra: list[Path]) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     return any(p.stat().st_mtime > t for p in sources() + _headers() + extra)
 
 
-def _compile(src: Path, verbose: bool) -> Path:
-    obj = BUILD / (src.name + ".o")
-    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-x", "cu", "-c", str(src), "-o", str(obj)]
+def _compile(src: Path, verbose: bool, checked: bool = False) -> Path:
+    obj = (BUILD_CHECKED if checked else BUILD) / (src.name + ".o")
+    extra = ["-DNNB_CHECKED"] if checked else []
+    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-x", "cu", "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -76,16 +85,18 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compiles and links the library; returns its path."""
-    if not force and not _stale([Path(__file__)]):
-        return LIB
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> Path:
+    """Compiles and links the library (the checked variant with checked=True); returns its
+    path."""
+    lib = LIB_CHECKED if checked else LIB
+    if not force and not _stale(lib, [Path(__file__)]):
+        return lib
+    (BUILD_CHECKED if checked else BUILD).mkdir(exist_ok=True)
     srcs = sources()
     workers = max(1, min(len(srcs), os.cpu_count() or 4))
     with cf.ThreadPoolExecutor(workers) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
-    tmp = LIB.with_suffix(".so.tmp")
+        objs = list(ex.map(lambda s: _compile(s, verbose, checked), srcs))
+    tmp = lib.with_suffix(".so.tmp")
     cmd = [_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs),
            "-cudart", "static", "-L", str(_cuda_lib_dir()), "-lcufft",
            "-Xlinker", "-rpath," + str(_cuda_lib_dir())]
@@ -94,16 +105,17 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--checked", action="store_true")
     a = ap.parse_args()
-    print(build(force=a.force, verbose=a.verbose))
+    print(build(force=a.force, verbose=a.verbose, checked=a.checked))
     return 0
 
 

@@ -112,7 +112,10 @@ __global__ void __launch_bounds__(kBinBlock)
     u32 r[kBinUnroll];
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
-      if (base + u * stride < M) r[u] = atomicAdd(&counts[tile_lin[u]], 1u);
+      if (base + u * stride < M) {
+        r[u] = NNB_CHECK_INDEX(tile_lin[u], g.total_tiles) ? atomicAdd(&counts[tile_lin[u]], 1u)
+                                                           : 0u;
+      }
     }
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
@@ -174,11 +177,14 @@ __global__ void __launch_bounds__(kBinBlock)
     u32 pos[kBinUnroll];
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
-      if (base + u * stride < M) pos[u] = bin_start[tile_lin[u]] + rank[u];
+      if (base + u * stride < M) {
+        pos[u] = NNB_CHECK_INDEX(tile_lin[u], g.total_tiles) ? bin_start[tile_lin[u]] + rank[u]
+                                                             : u32(M);
+      }
     }
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
-      if (base + u * stride < M) store_rec(&recs[pos[u]], r[u]);
+      if (base + u * stride < M && NNB_CHECK_INDEX(pos[u], M)) store_rec(&recs[pos[u]], r[u]);
     }
   }
 }

@@ -28,6 +28,7 @@ template <typename F>
 NeonufftError guard(F&& f) noexcept {
   try {
     f();
+    nnb::check_device_records();  // checked build only: synchronise, report failed checks
     return NEONUFFT_SUCCESS;
   } catch (const neonufft::GenericError& e) {
     t_last_error = e.what();
@@ -187,6 +188,14 @@ NeonufftError nnb_mlp_adam(int64_t n, float* params, const float* grads, float* 
 const char* nnb_version(void) { return "neonufft_b200 0.1.0 (sm_100a)"; }
 
 int64_t nnb_kernel_launches(void) { return nnb::g_kernel_launches.load(); }
+
+int nnb_is_checked_build(void) {
+#ifdef NNB_CHECKED
+  return 1;
+#else
+  return 0;
+#endif
+}
 
 NeonufftError nnb_device_alloc(void** ptr, size_t size) {
   return guard([&] {

@@ -73,6 +73,61 @@ void count_launch();
   } while (0)
 
 // ---------------------------------------------------------------------------------------------
+// Checked build (-DNNB_CHECKED): device bounds checks on every grid, record and output index of
+// the spreading, interpolation, deconvolution and binning kernels. A failed check skips the
+// access and records (first failure only) the source line, the index and its bound in this
+// translation unit's device record; it never traps, so the context stays usable. After every
+// C ABI call the checked build synchronises the device and reports a recorded failure as
+// InternalError (check_device_records, runtime.cu), the counterpart of the reference's debug
+// sync-and-check after each launch (src/neonufft/gpu/util/runtime.hpp:27-30). In the normal
+// build NNB_CHECK_INDEX is the constant true and the checks compile away.
+// ---------------------------------------------------------------------------------------------
+struct CheckRecord {
+  int flag;
+  int line;
+  long long index;
+  long long bound;
+};
+using CheckReadFn = CheckRecord (*)();
+// Registers a translation unit's reader and clearer of its device record (host, at load).
+bool register_check_record(CheckReadFn read, void (*clear)(), const char* unit);
+// Synchronises the device and throws InternalError if any unit recorded a failed check
+// (checked build; a no-op otherwise).
+void check_device_records();
+
+#ifdef NNB_CHECKED
+namespace {
+__device__ CheckRecord g_unit_check;
+CheckRecord read_unit_check() {
+  CheckRecord r{};
+  if (cudaMemcpyFromSymbol(&r, g_unit_check, sizeof(r)) != cudaSuccess) r.flag = 0;
+  return r;
+}
+void clear_unit_check() {
+  const CheckRecord z{};
+  (void)cudaMemcpyToSymbol(g_unit_check, &z, sizeof(z));
+}
+[[maybe_unused]] const bool g_unit_check_registered =
+    register_check_record(&read_unit_check, &clear_unit_check, __BASE_FILE__);
+__device__ __noinline__ void record_failed_check(long long i, long long n, int line) {
+  if (atomicCAS(&g_unit_check.flag, 0, 1) == 0) {
+    g_unit_check.line = line;
+    g_unit_check.index = i;
+    g_unit_check.bound = n;
+  }
+}
+}  // namespace
+__device__ __forceinline__ bool checked_index(long long i, long long n, int line) {
+  if (i >= 0 && i < n) return true;
+  record_failed_check(i, n, line);
+  return false;
+}
+#define NNB_CHECK_INDEX(i, n) (::nnb::checked_index((long long)(i), (long long)(n), __LINE__))
+#else
+#define NNB_CHECK_INDEX(i, n) true
+#endif
+
+// ---------------------------------------------------------------------------------------------
 // Geometry of a binned point set on a fine grid.
 //
 // Points are rescaled to p = frac(((x - offset) * scale + pi) / 2pi) in [0, 1), placed at

@@ -27,6 +27,14 @@ __device__ __forceinline__ i64 index_of_mode(i64 k, i64 n, int order) {
   return k >= 0 ? k : k + n;
 }
 
+// Elements spanned by the user's strided mode array: 1 + sum_d (modes_d - 1) stride_d.
+template <typename T>
+__device__ __forceinline__ i64 mode_array_extent(const DeconvArgs<T>& a) {
+  i64 e = 1;
+  for (int d = 0; d < a.dim; ++d) e += (a.modes[d] - 1) * a.stride[d];
+  return e;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kDeconvThreads)
     downsample_kernel(DeconvArgs<T> a, const cplx_t<T>* __restrict__ fine,
@@ -50,6 +58,10 @@ __global__ void __launch_bounds__(kDeconvThreads)
     c *= a.corr[2][k2 < 0 ? -k2 : k2];
     f += (k2 >= 0 ? k2 : a.nf[2] + k2) * a.nf[0] * a.nf[1];
     o += i2 * a.stride[2];
+  }
+  if (!NNB_CHECK_INDEX(f, a.nf[0] * a.nf[1] * a.nf[2]) ||
+      !NNB_CHECK_INDEX(o, mode_array_extent(a))) {
+    return;
   }
   const cplx_t<T> v = fine[f];
   out[o] = cplx_t<T>{v.x * c, v.y * c};
@@ -89,10 +101,12 @@ __global__ void __launch_bounds__(kDeconvThreads)
     c *= a.corr[d][k < 0 ? -k : k];
     src += index_of_mode(k, n, a.order) * a.stride[d];
   }
+  if (!NNB_CHECK_INDEX(f, a.nf[0] * a.nf[1] * a.nf[2])) return;
   if (!inside) {
     fine[f] = cplx_t<T>{T(0), T(0)};
     return;
   }
+  if (!NNB_CHECK_INDEX(src, mode_array_extent(a))) return;
   const cplx_t<T> v = in[src];
   fine[f] = cplx_t<T>{v.x * c, v.y * c};
 }

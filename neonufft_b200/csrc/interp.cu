@@ -35,7 +35,8 @@ __device__ __forceinline__ void stage_region(const BinGeom& g, const TileLayout&
     (void)o1;
     (void)o2;
     for (int cx = threadIdx.x; cx < ext1d; cx += blockDim.x) {
-      tile[cx] = grid[wrap_index(o0 + cx, g.nf[0])];
+      const i64 gi = wrap_index(o0 + cx, g.nf[0]);
+      tile[cx] = NNB_CHECK_INDEX(gi, g.nf[0]) ? grid[gi] : cplx_t<T>{T(0), T(0)};
     }
   } else {
     (void)ext1d;
@@ -52,7 +53,9 @@ __device__ __forceinline__ void stage_region(const BinGeom& g, const TileLayout&
       if (DIM == 3) rbase += wrap_index(o2 + cz, g.nf[2]) * g.nf[0] * g.nf[1];
       cplx_t<T>* dst = tile + cz * L.PS + cy * L.RS;
       for (int cx = lane; cx < L.P0; cx += 32) {
-        dst[cx] = grid[rbase + wrap_index(o0 + cx, g.nf[0])];
+        const i64 gi = rbase + wrap_index(o0 + cx, g.nf[0]);
+        dst[cx] = NNB_CHECK_INDEX(gi, g.nf[0] * g.nf[1] * g.nf[2]) ? grid[gi]
+                                                                   : cplx_t<T>{T(0), T(0)};
       }
     }
   }
@@ -140,10 +143,10 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
     int my_base = 0;
     u32 my_idx = 0;
     C my_post{T(1), T(0)};
-    if (lane < nb) {
+    if (lane < nb && NNB_CHECK_INDEX(i64(b) + lane, a.pts.M)) {
       const PointRec<T> rec = a.pts.rec[b + lane];
       my_idx = rec.perm;
-      if (a.postphase) my_post = a.postphase[my_idx];
+      if (a.postphase && NNB_CHECK_INDEX(my_idx, a.pts.M)) my_post = a.postphase[my_idx];
       int lx, ly, lz;
       unpack_local(DIM, rec.local, lx, ly, lz);
       my_base = shift + lz * L.PS + ly * L.RS + lx;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kMaxInterpWarps * 32) interp_slab_kernel(Inter
       if (lane == int(j)) {
         C res{sx, sy};
         if (a.postphase) res = cmul(res, my_post);
-        a.out[my_idx] = res;
+        if (NNB_CHECK_INDEX(my_idx, a.pts.M)) a.out[my_idx] = res;
       }
     }
     __syncwarp();
@@ -233,6 +236,7 @@ __global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a
                        t1 * g.tile[1], t2 * g.tile[2], a.grid, tile);
   __syncthreads();
   for (u32 p = start + threadIdx.x; p < end; p += kTppThreads) {
+    if (!NNB_CHECK_INDEX(p, a.pts.M)) break;
     const PointRec<T> rec = a.pts.rec[p];
     int lx, ly, lz;
     unpack_local(DIM, rec.local, lx, ly, lz);
@@ -265,6 +269,7 @@ __global__ void __launch_bounds__(kTppThreads) interp_tpp_kernel(InterpArgs<T> a
     }
     const u32 idx = rec.perm;
     C res{sx, sy};
+    if (!NNB_CHECK_INDEX(idx, a.pts.M)) continue;
     if (a.postphase) res = cmul(res, a.postphase[idx]);
     a.out[idx] = res;
   }

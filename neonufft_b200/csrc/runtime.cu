@@ -1,6 +1,7 @@
 // Host runtime: errors, allocator adapter, stage timer, cuFFT grid, point sets, tile choice.
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "runtime.hpp"
 
@@ -9,6 +10,52 @@ namespace nnb {
 std::atomic<i64> g_kernel_launches{0};
 
 void count_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
+const char* stage_range_name(int stage) {
+  static const char* const names[] = {"nnb:bin", "nnb:spread", "nnb:fft", "nnb:deconv",
+                                      "nnb:interp", "nnb:phase"};
+  return (stage >= 0 && stage < int(sizeof(names) / sizeof(names[0]))) ? names[stage] : "nnb";
+}
+
+namespace {
+struct CheckUnit {
+  CheckReadFn read;
+  void (*clear)();
+  const char* name;
+};
+std::vector<CheckUnit>& check_units() {
+  static std::vector<CheckUnit> units;  // filled during static initialisation of the library
+  return units;
+}
+}  // namespace
+
+bool register_check_record(CheckReadFn read, void (*clear)(), const char* unit) {
+  check_units().push_back(CheckUnit{read, clear, unit});
+  return true;
+}
+
+void check_device_records() {
+#ifdef NNB_CHECKED
+  // Never synchronise while a stream capture is open (the checked build is for uncaptured
+  // debugging runs): the legacy stream reports one, or refuses the query during it.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(cudaStreamLegacy, &cap) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  if (cap != cudaStreamCaptureStatusNone) return;
+  NNB_CUDA(cudaDeviceSynchronize());
+  for (const CheckUnit& u : check_units()) {
+    const CheckRecord r = u.read();
+    if (r.flag) {
+      u.clear();
+      throw_internal(std::string("checked build: index ") + std::to_string(r.index) +
+                     " outside [0, " + std::to_string(r.bound) + ") at " + u.name + ":" +
+                     std::to_string(r.line));
+    }
+  }
+#endif
+}
 
 // ---- errors -----------------------------------------------------------------------------------
 namespace {

@@ -6,6 +6,8 @@
 #include <memory>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "neonufft_gpu.h"
@@ -93,12 +95,21 @@ private:
   i64 count_[NNB_STAGE_COUNT] = {0};
 };
 
+// One stage of a transform: an NVTX range on the host thread named after the stage ("nnb:bin",
+// "nnb:spread", "nnb:fft", "nnb:deconv", "nnb:interp", "nnb:phase"; visible in Nsight Systems and
+// as ncu's --nvtx ranges, free when no tool is attached) and, when timing is on, CUDA events
+// around the stage's launches.
+const char* stage_range_name(int stage);
 class ScopedStage {
 public:
   ScopedStage(StageTimer& t, cudaStream_t s, int stage) : t_(t), s_(s), stage_(stage) {
+    nvtxRangePushA(stage_range_name(stage_));
     t_.begin(s_, stage_);
   }
-  ~ScopedStage() { t_.end(s_, stage_); }
+  ~ScopedStage() {
+    t_.end(s_, stage_);
+    nvtxRangePop();
+  }
 
 private:
   StageTimer& t_;

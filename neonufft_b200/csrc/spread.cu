@@ -63,7 +63,8 @@ __device__ __forceinline__ void writeback_rows(const BinGeom& g, const TileLayou
     for (int cx = lane; cx < L.P0; cx += 32) {
       const cplx_t<T> val = src[cx];
       if (val.x == T(0) && val.y == T(0)) continue;
-      atomic_add_cplx(&grid[rbase + wrap_index(o0 + cx, g.nf[0])], val);
+      const i64 gi = rbase + wrap_index(o0 + cx, g.nf[0]);
+      if (NNB_CHECK_INDEX(gi, g.nf[0] * g.nf[1] * g.nf[2])) atomic_add_cplx(&grid[gi], val);
     }
   }
 }
@@ -148,11 +149,13 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
       const u32 nb = (end - b) < 32u ? (end - b) : 32u;
       int my_base = 0;
       C my_v{T(0), T(0)};
-      if (lane < nb) {
+      if (lane < nb && NNB_CHECK_INDEX(i64(b) + lane, a.pts.M)) {
         const PointRec<T> rec = a.pts.rec[b + lane];
         const u32 idx = rec.perm;
-        my_v = in[idx];
-        if (a.prephase) my_v = cmul(my_v, a.prephase[idx]);
+        if (NNB_CHECK_INDEX(idx, a.pts.M)) {
+          my_v = in[idx];
+          if (a.prephase) my_v = cmul(my_v, a.prephase[idx]);
+        }
         int lx, ly, lz;
         unpack_local(DIM, rec.local, lx, ly, lz);
         my_base = lz * L.PS + ly * L.RS + lx;
@@ -292,7 +295,8 @@ __global__ void __launch_bounds__(kMaxSlabWarps * 32) spread_slab_kernel(SpreadA
       for (int cx = threadIdx.x; cx < planes; cx += blockDim.x) {
         const C val = slab[cx];
         if (val.x == T(0) && val.y == T(0)) continue;
-        atomic_add_cplx(&grid[wrap_index(ox + cx, g.nf[0])], val);
+        const i64 gi = wrap_index(ox + cx, g.nf[0]);
+        if (NNB_CHECK_INDEX(gi, g.nf[0])) atomic_add_cplx(&grid[gi], val);
       }
     }
   }
@@ -320,8 +324,10 @@ __global__ void __launch_bounds__(kTppThreads) spread_tpp_kernel(SpreadArgs<T> a
   __syncthreads();
 
   for (u32 p = start + threadIdx.x; p < end; p += kTppThreads) {
+    if (!NNB_CHECK_INDEX(p, a.pts.M)) break;
     const PointRec<T> rec = a.pts.rec[p];
     const u32 idx = rec.perm;
+    if (!NNB_CHECK_INDEX(idx, a.pts.M)) continue;
     C v = in[idx];
     if (a.prephase) v = cmul(v, a.prephase[idx]);
     int lx, ly, lz;
@@ -360,7 +366,8 @@ __global__ void __launch_bounds__(kTppThreads) spread_tpp_kernel(SpreadArgs<T> a
     for (int cx = threadIdx.x; cx < L.P0; cx += kTppThreads) {
       const C val = acc[cx];
       if (val.x == T(0) && val.y == T(0)) continue;
-      atomic_add_cplx(&grid[wrap_index(t0 * g.tile[0] + cx, g.nf[0])], val);
+      const i64 gi = wrap_index(t0 * g.tile[0] + cx, g.nf[0]);
+      if (NNB_CHECK_INDEX(gi, g.nf[0])) atomic_add_cplx(&grid[gi], val);
     }
   } else {
     writeback_rows<T, DIM>(g, L, acc, L.P1 * L.P2, t0 * g.tile[0], t1 * g.tile[1],

@@ -171,7 +171,8 @@ struct alignas(16) ZSlot
 template <typename T, int W, int TX, bool SPREAD, int TY = 8>
 __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX, TY>* slots, const PointRec<T>* recs,
                                            int count, const cplx_t<T>* in,
-                                           const cplx_t<T>* prephase, T beta, T c, int lane) {
+                                           const cplx_t<T>* prephase, T beta, T c, int lane,
+                                           i64 num) {
   using S = ZShape<T, W, TX, TY>;
   using C = cplx_t<T>;
   constexpr unsigned kFull = 0xffffffffu;
@@ -183,8 +184,10 @@ __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX, TY>* slots, const Poi
   if (lane < count) {
     rec = recs[lane];
     if constexpr (SPREAD) {
-      v = in[rec.perm];
-      if (prephase) v = cmul(v, prephase[rec.perm]);
+      if (NNB_CHECK_INDEX(rec.perm, num)) {
+        v = in[rec.perm];
+        if (prephase) v = cmul(v, prephase[rec.perm]);
+      }
     }
   }
   const int p = lane >> 1;
@@ -331,6 +334,7 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
+  [[maybe_unused]] const i64 cells = nfx * nfy * nfz;
   const bool narrow = nfx < S::P0;
   const bool has_row = th.ra < S::P1;
   const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
@@ -348,15 +352,18 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
                      (reinterpret_cast<size_t>(grid) % 16) == 0;
   auto flush = [&](int p) {
     if (has_row && dirty) {
-      C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+      const i64 base = (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+      C* row = grid + base;
       if (pairs) {
         C* r = row + gx0;
 #pragma unroll
         for (int q = 0; q < S::NP; ++q) {
           if (2 * q + 1 < S::P0) {
-            atomic_add_pair(r + 2 * q, Ops::lo(are[q]), Ops::lo(aim[q]), Ops::hi(are[q]),
-                            Ops::hi(aim[q]));
-          } else {
+            if (NNB_CHECK_INDEX(base + gx0 + 2 * q + 1, cells)) {
+              atomic_add_pair(r + 2 * q, Ops::lo(are[q]), Ops::lo(aim[q]), Ops::hi(are[q]),
+                              Ops::hi(aim[q]));
+            }
+          } else if (NNB_CHECK_INDEX(base + gx0 + 2 * q, cells)) {
             atomic_add_cplx(r + 2 * q, C{Ops::lo(are[q]), Ops::lo(aim[q])});
           }
           are[q] = aim[q] = Ops::zero();
@@ -364,11 +371,13 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
       } else {
 #pragma unroll
         for (int q = 0; q < S::NP; ++q) {
-          atomic_add_cplx(&row[wrap_x(gx0, 2 * q, nfx, narrow)],
-                          C{Ops::lo(are[q]), Ops::lo(aim[q])});
-          if (2 * q + 1 < S::P0) {
-            atomic_add_cplx(&row[wrap_x(gx0, 2 * q + 1, nfx, narrow)],
-                            C{Ops::hi(are[q]), Ops::hi(aim[q])});
+          const i64 x0 = wrap_x(gx0, 2 * q, nfx, narrow);
+          if (NNB_CHECK_INDEX(base + x0, cells)) {
+            atomic_add_cplx(&row[x0], C{Ops::lo(are[q]), Ops::lo(aim[q])});
+          }
+          const i64 x1 = wrap_x(gx0, 2 * q + 1, nfx, narrow);
+          if (2 * q + 1 < S::P0 && NNB_CHECK_INDEX(base + x1, cells)) {
+            atomic_add_cplx(&row[x1], C{Ops::hi(are[q]), Ops::hi(aim[q])});
           }
           are[q] = aim[q] = Ops::zero();
         }
@@ -385,9 +394,14 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
     constexpr int PW = S::BATCH / S::NWARP;  // points per warp
     const int count = min(nb - th.warp * PW, PW);
     for (int c0 = 0; c0 < count; c0 += 16) {
+      if (!NNB_CHECK_INDEX(i64(cta.pbeg) + off + th.warp * PW + c0 + min(count - c0, 16) - 1,
+                           a.pts.M)) {
+        break;
+      }
       stage_warp<T, W, TX, true, TY>(slots[k & 1] + th.warp * PW + c0,
                                  a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
-                                 min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane);
+                                 min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane,
+                                 a.pts.M);
     }
   };
 
@@ -593,8 +607,10 @@ __global__ void __launch_bounds__(128) spread_zmma_kernel(SpreadArgs<float> a, Z
           const int y = 8 * yg + 2 * tq + (e & 1);
           if (x < S::P0 && y < S::P1) {
             const i64 gy = wrap_add(gy0, y, nfy);
-            atomic_add_cplx(&grid[(plane * nfy + gy) * nfx + wrap_x(gx0, x, nfx, narrow)],
-                            C{cre[pl][yg][e], cim[pl][yg][e]});
+            const i64 idx = (plane * nfy + gy) * nfx + wrap_x(gx0, x, nfx, narrow);
+            if (NNB_CHECK_INDEX(idx, nfx * nfy * nfz)) {
+              atomic_add_cplx(&grid[idx], C{cre[pl][yg][e], cim[pl][yg][e]});
+            }
           }
           cre[pl][yg][e] = cim[pl][yg][e] = 0.f;
         }
@@ -615,9 +631,14 @@ __global__ void __launch_bounds__(128) spread_zmma_kernel(SpreadArgs<float> a, Z
     constexpr int PW = S::BATCH / S::NWARP;
     const int count = min(nb - th.warp * PW, PW);
     for (int c0 = 0; c0 < count; c0 += 16) {
+      if (!NNB_CHECK_INDEX(i64(cta.pbeg) + off + th.warp * PW + c0 + min(count - c0, 16) - 1,
+                           a.pts.M)) {
+        break;
+      }
       stage_warp<float, W, TX, true>(slots[k & 1] + th.warp * PW + c0,
                                      a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
-                                     min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane);
+                                     min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane,
+                                     a.pts.M);
     }
   };
 
@@ -705,6 +726,7 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
   const ZThread<T, W, TX, TY> th;
   const C* grid = a.grid;
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
+  [[maybe_unused]] const i64 cells = nfx * nfy * nfz;
   const bool narrow = nfx < S::P0;
   const bool has_row = th.ra < S::P1;
   const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
@@ -722,17 +744,22 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
                        (reinterpret_cast<size_t>(grid) % 16) == 0;
   auto load_row = [&](int p) {
     if (!has_row) return;
-    const C* row = grid + (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+    const i64 base = (wrap_plane(p, nfz) * nfy + row_y) * nfx;
+    const C* row = grid + base;
     if constexpr (sizeof(T) == 4) {
       if (pairs16) {
 #pragma unroll
         for (int q = 0; q < S::NP; ++q) {
           if (2 * q + 1 < S::P0) {
-            const float4 v = *reinterpret_cast<const float4*>(row + gx0 + 2 * q);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (NNB_CHECK_INDEX(base + gx0 + 2 * q + 1, cells)) {
+              v = *reinterpret_cast<const float4*>(row + gx0 + 2 * q);
+            }
             gre[q] = Ops::pack(v.x, v.z);
             gim[q] = Ops::pack(v.y, v.w);
           } else {
-            const C c0 = row[gx0 + 2 * q];
+            C c0{T(0), T(0)};
+            if (NNB_CHECK_INDEX(base + gx0 + 2 * q, cells)) c0 = row[gx0 + 2 * q];
             gre[q] = Ops::pack(c0.x, T(0));
             gim[q] = Ops::pack(c0.y, T(0));
           }
@@ -742,14 +769,11 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
     }
 #pragma unroll
     for (int q = 0; q < S::NP; ++q) {
-      C c0, c1{T(0), T(0)};
-      if (contiguous) {
-        c0 = row[gx0 + 2 * q];
-        if (2 * q + 1 < S::P0) c1 = row[gx0 + 2 * q + 1];
-      } else {
-        c0 = row[wrap_x(gx0, 2 * q, nfx, narrow)];
-        if (2 * q + 1 < S::P0) c1 = row[wrap_x(gx0, 2 * q + 1, nfx, narrow)];
-      }
+      C c0{T(0), T(0)}, c1{T(0), T(0)};
+      const i64 x0 = contiguous ? gx0 + 2 * q : wrap_x(gx0, 2 * q, nfx, narrow);
+      const i64 x1 = contiguous ? gx0 + 2 * q + 1 : wrap_x(gx0, 2 * q + 1, nfx, narrow);
+      if (NNB_CHECK_INDEX(base + x0, cells)) c0 = row[x0];
+      if (2 * q + 1 < S::P0 && NNB_CHECK_INDEX(base + x1, cells)) c1 = row[x1];
       gre[q] = Ops::pack(c0.x, c1.x);
       gim[q] = Ops::pack(c0.y, c1.y);
     }
@@ -762,9 +786,14 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
     constexpr int PW = S::BATCH / S::NWARP;  // points per warp
     const int count = min(nb - th.warp * PW, PW);
     for (int c0 = 0; c0 < count; c0 += 16) {
+      if (!NNB_CHECK_INDEX(i64(cta.pbeg) + off + th.warp * PW + c0 + min(count - c0, 16) - 1,
+                           a.pts.M)) {
+        break;
+      }
       stage_warp<T, W, TX, false, TY>(slots[k & 1] + th.warp * PW + c0,
                                   a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
-                                  min(count - c0, 16), nullptr, nullptr, a.beta, a.c, th.lane);
+                                  min(count - c0, 16), nullptr, nullptr, a.beta, a.c, th.lane,
+                                  a.pts.M);
     }
   };
   // Writes the outputs of batch k: this thread's staged point, whose slot only this thread's
@@ -780,8 +809,10 @@ __device__ __forceinline__ void interp_zwin_item(const InterpArgs<T>& a, ZChunks
         r.y += res[k & 1][w][j].y;
       }
       const u32 perm = slots[k & 1][j].perm;
-      if (a.postphase) r = cmul(r, a.postphase[perm]);
-      a.out[perm] = r;
+      if (NNB_CHECK_INDEX(perm, a.pts.M)) {
+        if (a.postphase) r = cmul(r, a.postphase[perm]);
+        a.out[perm] = r;
+      }
     }
   };
 
