@@ -1035,6 +1035,8 @@ def main():
     ap.add_argument("--points", type=int, default=0,
                     help="override the workload's point count M (small ncu captures of the same "
                          "grid); the line records the M it ran")
+    ap.add_argument("--modes", type=int, default=0,
+                    help="override the workload's modes per dimension N (small ncu captures)")
     ap.add_argument("--ref-steps", type=int, default=3,
                     help="timed steps of the reference GPU plan arm (at most --steps)")
     ap.add_argument("--spread-method", type=int, default=0,
@@ -1054,6 +1056,8 @@ def main():
     if args.points > 0 and "M" in wl:
         wl["M"] = args.points
         wl["cpu_sample"] = min(wl.get("cpu_sample", args.points), args.points)
+    if args.modes > 0 and "N" in wl:
+        wl["N"] = args.modes
     if args.impl == "reference":
         if "batch" in wl or "tuner" in wl or "t3" in wl:
             print(json.dumps({"impl": "reference", "unavailable":

@@ -63,7 +63,10 @@ typedef struct NnbOptions {
                                1 = warp-private shared-memory slabs; 2 = thread per point;
                                3 = sliding z-window held in registers (3D, width <= 8);
                                4 = method 3 with the row updates on the tensor cores (TF32 with
-                               split operands; 3D, single precision, width 5 to 8) */
+                               split operands; 3D, single precision, width 5 to 8);
+                               5 = spreading on the tcgen05 tensor cores with the region's
+                               accumulator in tensor memory (3D, single precision, width <= 8,
+                               tiles {4, 4, 1}); interpolation as method 3 */
   int n_spread;             /* kernel width override in [2, 16]; 0 = the reference heuristic */
   int reserved[7];
 } NnbOptions;
@@ -347,6 +350,14 @@ NNB_API NeonufftError nnb_mlp_adam(int64_t n, float* params, const float* grads,
  * counterpart is its debug-build sync-and-check after each launch
  * (src/neonufft/gpu/util/runtime.hpp:27-30). */
 NNB_API int nnb_is_checked_build(void);
+
+/* Synchronises the current device and reads the engine's device status: NEONUFFT_GPU_ERROR (with
+ * a message) if a bounded wait inside an engine kernel gave up since the last call -- the
+ * tensor-core spreading (spread method 5) waits at most 2 s for its matrix products, then
+ * abandons the work item, frees its tensor memory and records the failure here instead of
+ * hanging -- else NEONUFFT_SUCCESS. The status is cleared by the call. Engine extension; the
+ * reference has no device-side waits. */
+NNB_API NeonufftError nnb_check_device_status(void);
 NNB_API const char* nnb_version(void);
 
 /* Number of engine kernels this process has launched so far (all plans and devices; cuFFT's

@@ -6,10 +6,12 @@ over that ABI; it contains no numerical fallback.
 """
 from .plan import (MODE_ORDER_CMCL, MODE_ORDER_FFT, Batch, GenericError, GPUError, InputError,
                    InternalError, MemoryAllocError, NotImplementedError_, Options, Plan, PlanT3,
-                   direct_type1_f64, direct_type2_f64, direct_type3_f64, kernel_launches)
+                   check_device_status, direct_type1_f64, direct_type2_f64, direct_type3_f64,
+                   kernel_launches)
 
 __all__ = [
     "Options", "Plan", "PlanT3", "Batch", "MODE_ORDER_CMCL", "MODE_ORDER_FFT", "GenericError",
     "GPUError", "InputError", "InternalError", "MemoryAllocError", "NotImplementedError_",
     "direct_type1_f64", "direct_type2_f64", "direct_type3_f64", "kernel_launches",
+    "check_device_status",
 ]

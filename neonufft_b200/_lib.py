@@ -103,6 +103,7 @@ SIGNATURES = [
     ("nnb_version", C.c_char_p, []),
     ("nnb_kernel_launches", C.c_int64, []),
     ("nnb_is_checked_build", C.c_int, []),
+    ("nnb_check_device_status", _E, []),
 ]
 
 _lib = None

@@ -189,6 +189,16 @@ const char* nnb_version(void) { return "neonufft_b200 0.1.0 (sm_100a)"; }
 
 int64_t nnb_kernel_launches(void) { return nnb::g_kernel_launches.load(); }
 
+NeonufftError nnb_check_device_status(void) {
+  return guard([&] {
+    NNB_CUDA(cudaDeviceSynchronize());
+    if (nnb::read_tc_status(true)) {
+      throw neonufft::GPUError(
+          "Neonufft:: tensor-core spreading: a bounded wait for the matrix products gave up");
+    }
+  });
+}
+
 int nnb_is_checked_build(void) {
 #ifdef NNB_CHECKED
   return 1;

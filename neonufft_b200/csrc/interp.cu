@@ -353,7 +353,8 @@ size_t interp_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, 
 template <typename T>
 void launch_interp(const InterpArgs<T>& a, cudaStream_t stream) {
   if (a.g.total_tiles <= 0) return;
-  if (a.method == 3 || a.method == 4) return launch_interp_zwin<T>(a, stream);
+  // method 5 spreads on the tensor cores; it interpolates with the z-window kernel
+  if (a.method == 3 || a.method == 4 || a.method == 5) return launch_interp_zwin<T>(a, stream);
   switch (a.g.dim) {
     case 1: return launch_interp_d<T, 1>(a, stream);
     case 2: return launch_interp_d<T, 2>(a, stream);

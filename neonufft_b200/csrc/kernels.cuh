@@ -86,6 +86,11 @@ template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream);
 template <typename T>
 void launch_spread_zwin(const SpreadArgs<T>& a, cudaStream_t stream);
+// Method 5: 3D single-precision spreading on the tcgen05 tensor cores (spread_tc.cu).
+void launch_spread_tc(const SpreadArgs<float>& a, cudaStream_t stream);
+// Status word of the tensor-core spreading: nonzero once one of its bounded waits gave up
+// (synchronous read; clear resets it).
+int read_tc_status(bool clear);
 // Dynamic shared memory of the default spreading / interpolation kernels for a tile shape.
 size_t spread_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
 size_t interp_smem_bytes(int dim, int w, const int* tile, size_t complex_bytes, int warps);
@@ -114,6 +119,13 @@ struct ZChunks {
   int len;    // planes per chunk
   int count;  // chunks per column
 };
+// Chunks of `len` planes for ncols columns of nz planes (at least 4 w planes each), and the work
+// list of a plane-major point set's (column, chunk) units (zwin.cu; also used by the
+// tensor-core spreading, spread_tc.cu).
+ZChunks make_chunks(i64 ncols, int nz, int w);
+template <typename T>
+WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch,
+                        cudaStream_t stream);
 // One transform's share of a persistent launch: its arguments, chunks and work list.
 template <typename T>
 struct ZSpreadJob {

@@ -68,7 +68,7 @@ void validate_options(const NnbOptions& opt) {
   for (int d = 0; d < 3; ++d) {
     if (opt.tile[d] < 0) throw_input("invalid tile shape");
   }
-  if (opt.spread_method < 0 || opt.spread_method > 4) throw_input("invalid spread method");
+  if (opt.spread_method < 0 || opt.spread_method > 5) throw_input("invalid spread method");
   if (opt.n_spread != 0 && (opt.n_spread < 2 || opt.n_spread > 16)) {
     throw_input("kernel width must be in [2, 16]");
   }

@@ -303,6 +303,10 @@ int choose_method(int dim, int w, int requested, bool single) {
   if (requested == 4 && (dim != 3 || w < 5 || w > 8 || !single)) {
     throw_input("spread method 4 needs a single-precision 3D plan with kernel width in [5, 8]");
   }
+  if (requested == 5 && (dim != 3 || w > 8 || !single)) {
+    throw_input("spread method 5 needs a single-precision 3D plan with kernel width <= 8");
+  }
+  if (requested < 0 || requested > 5) throw_input("spread method must be in [0, 5]");
   if (requested > 0) return requested;
   return (dim == 3 && w <= 8) ? 3 : 1;
 }
@@ -316,6 +320,16 @@ void choose_tile(int dim, int w, size_t complex_bytes, const i64* nf, const int*
     if (explicit_tile && requested[0] != 8) throw_input("spread method 4 uses tiles of 8 x 8 x 1");
     tile[0] = 8;
     tile[1] = 8;
+    tile[2] = 1;
+    return;
+  }
+  if (method == 5) {
+    // the tensor-core spreading's accumulator rows are the (4 + w - 1)^2 <= 121 region cells
+    if (explicit_tile && (requested[0] != 4 || (requested[1] != 0 && requested[1] != 4))) {
+      throw_input("spread method 5 uses tiles of 4 x 4 x 1");
+    }
+    tile[0] = 4;
+    tile[1] = 4;
     tile[2] = 1;
     return;
   }

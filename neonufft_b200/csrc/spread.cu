@@ -19,6 +19,8 @@
 //    region is added to the global grid once, coalesced along x, with float2/double2 atomics
 //    (regions of neighbouring CTAs overlap by the halo).
 // Method 2, thread per point with shared-memory atomics, is kept as an alternative.
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "tile_layout.cuh"
 
@@ -453,6 +455,10 @@ template <typename T>
 void launch_spread(const SpreadArgs<T>& a, cudaStream_t stream) {
   if (a.g.total_tiles <= 0 || a.batch <= 0) return;
   if (a.method == 3 || a.method == 4) return launch_spread_zwin<T>(a, stream);
+  if (a.method == 5) {
+    if constexpr (std::is_same<T, float>::value) return launch_spread_tc(a, stream);
+    throw_internal("tensor-core spreading is single precision");
+  }
   switch (a.g.dim) {
     case 1: return launch_spread_d<T, 1>(a, stream);
     case 2: return launch_spread_d<T, 2>(a, stream);

@@ -937,6 +937,8 @@ __global__ void __launch_bounds__(ZShape<T, W, TX>::NT, kInterpFusedCtas<T>)
   }
 }
 
+}  // namespace
+
 ZChunks make_chunks(i64 ncols, int nz, int w) {
   // About four waves of 8 CTAs per SM; chunks of at least 4 w planes bound the window
   // overhead (w - 1 extra planes flushed, or RZ planes loaded, per chunk).
@@ -976,6 +978,12 @@ WorkList zwin_work_list(const BinGeom& g, const SortedPoints<T>& pts, ZChunks ch
   if (wl.grid > 0x7fffffffll) throw_input("grid too large");
   return wl;
 }
+template WorkList zwin_work_list<float>(const BinGeom&, const SortedPoints<float>&, ZChunks,
+                                         cudaStream_t);
+template WorkList zwin_work_list<double>(const BinGeom&, const SortedPoints<double>&, ZChunks,
+                                          cudaStream_t);
+
+namespace {
 
 template <typename T, int W, int TX, int TY>
 void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {

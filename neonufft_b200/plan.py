@@ -421,3 +421,9 @@ def direct_type3_f64(sign: int, in_loc: Sequence, c, out_loc: Sequence, target_i
 def kernel_launches() -> int:
     """Engine kernel launches issued by this process so far."""
     return int(L.load().nnb_kernel_launches())
+
+
+def check_device_status() -> None:
+    """Synchronises the device; raises GPUError if a bounded wait inside an engine kernel gave
+    up since the last check (nnb_check_device_status)."""
+    check(L.load().nnb_check_device_status())
