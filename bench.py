@@ -1035,6 +1035,9 @@ def main():
     ap.add_argument("--points", type=int, default=0,
                     help="override the workload's point count M (small ncu captures of the same "
                          "grid); the line records the M it ran")
+    ap.add_argument("--extents", default="",
+                    help="type-3 half-widths X,S,X3,S3 (2D sources / targets, 3D sources / "
+                         "targets) overriding the workload's (small ncu captures)")
     ap.add_argument("--modes", type=int, default=0,
                     help="override the workload's modes per dimension N (small ncu captures)")
     ap.add_argument("--ref-steps", type=int, default=3,
@@ -1058,6 +1061,8 @@ def main():
         wl["cpu_sample"] = min(wl.get("cpu_sample", args.points), args.points)
     if args.modes > 0 and "N" in wl:
         wl["N"] = args.modes
+    if args.extents and "t3" in wl:
+        wl["X"], wl["S"], wl["X3"], wl["S3"] = (float(v) for v in args.extents.split(","))
     if args.impl == "reference":
         if "batch" in wl or "tuner" in wl or "t3" in wl:
             print(json.dumps({"impl": "reference", "unavailable":
