@@ -7,7 +7,8 @@ synchronises and reports a recorded failure as NEONUFFT_INTERNAL_ERROR -- the co
 reference's debug-build sync-and-check after each launch (src/neonufft/gpu/util/runtime.hpp:27-30).
 
 The GPU test runs the small-case parity suites (the reference's type-1/2 and type-3 matrices,
-every spreading method and tile, the edge cases and the batches) in a child process that loads
+every spreading method and tile including the tensor-core spreading, the edge cases and the
+batches) in a child process that loads
 the checked library, so that any out-of-range index in those kernels fails the run.
 """
 import os
@@ -45,7 +46,7 @@ def test_parity_suites_under_the_checked_build(cuda):
     if not CHECKED.exists():
         pytest.fail("the checked build is missing: python -m neonufft_b200.build --checked")
     suites = ["tests/test_gpu_type12.py", "tests/test_gpu_type3.py", "tests/test_gpu_methods.py",
-              "tests/test_gpu_edges.py", "tests/test_gpu_batch.py"]
+              "tests/test_gpu_tcgen05.py", "tests/test_gpu_edges.py", "tests/test_gpu_batch.py"]
     env = dict(os.environ, NEONUFFT_B200_LIB=str(CHECKED))
     res = subprocess.run([sys.executable, "-m", "pytest", "-m", "gpu", "-x", "-q",
                           "-p", "no:cacheprovider", *suites],
