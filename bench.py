@@ -583,15 +583,15 @@ def run_type3(args, wl):
 
 def load_traffic(workload, precision, kernel, w, tile):
     """DRAM bytes (read + write) of one launch of `kernel`, as a linear model a*M + b fitted to
-    ncu captures of the same configuration, from the committed summary profiles/dram_traffic.md
-    (rows '| workload | precision | kernel | w | tile | a | b |'). None when not captured."""
-    p = ROOT / "profiles" / "dram_traffic.md"
+    ncu captures of the same configuration (rows 'workload precision kernel w tile a b' of
+    profiles/dram_traffic_fit.txt). None when the configuration was not captured."""
+    p = ROOT / "profiles" / "dram_traffic_fit.txt"
     if not p.exists():
         return None
-    key = (workload, precision, kernel, str(w), ",".join(str(int(v)) for v in tile))
+    key = [workload, precision, kernel, str(w), ",".join(str(int(v)) for v in tile)]
     for line in p.read_text().splitlines():
-        cells = [x.strip() for x in line.strip().strip("|").split("|")]
-        if len(cells) >= 7 and tuple(cells[:5]) == key:
+        cells = line.split()
+        if len(cells) >= 7 and not line.lstrip().startswith("#") and cells[:5] == key:
             try:
                 return float(cells[5]), float(cells[6])
             except ValueError:
@@ -956,7 +956,7 @@ def run_transform(args, wl):
         "algorithmic_bytes_formula": "M (d + 2) s_T + 2 s_T nf^d",
         "launch_ms": dom_ms,
         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, linear fit a M + b "
-                           "from profiles/dram_traffic.md" if model else
+                           "from profiles/dram_traffic_fit.txt" if model else
                            "not captured for this configuration"),
         "fp32": {"achieved_tflops": alg_flop / (dom_ms * 1e-3) / 1e12,
                  "peak_tflops_nominal": fp32_peak,

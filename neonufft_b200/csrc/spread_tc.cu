@@ -37,7 +37,6 @@
 // of 8 rows (stride byte offset); the instruction descriptor gives the D / A / B formats
 // (F32 / TF32 / TF32), both operands K-major, N / 8 and M / 16 (the bit layout of the sm_100
 // UMMA descriptors as published in CUTLASS's cute/arch/mma_sm100_desc.hpp).
-#include <atomic>
 #include <cstdint>
 
 #include "common.cuh"
@@ -583,16 +582,10 @@ void launch_spread_tc_w(const SpreadArgs<float>& a, cudaStream_t stream) {
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
   const size_t smem = sizeof(TcShared<W>);
-  // the shared-memory limit is a per-device attribute of the function: set once per device
-  static std::atomic<unsigned long long> configured{0};
-  int dev = 0;
-  NNB_CUDA(cudaGetDevice(&dev));
-  const unsigned long long bit = 1ull << (dev & 63);
-  if (!(configured.load() & bit)) {
-    NNB_CUDA(cudaFuncSetAttribute(spread_tc_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem)));
-    configured.fetch_or(bit);
-  }
+  // the dynamic shared-memory limit is an attribute of the function on the current device; a
+  // host-side call per launch, so any device the caller switches to is covered
+  NNB_CUDA(cudaFuncSetAttribute(spread_tc_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(smem)));
   const dim3 grid{unsigned(wl.grid), unsigned(a.batch), 1u};
   spread_tc_kernel<W><<<grid, kTcThreads, smem, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();
