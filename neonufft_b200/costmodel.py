@@ -124,3 +124,24 @@ class CostModel:
 
     def predict(self, feats) -> np.ndarray:
         return self.net.predict(self._norm(feats)).cpu().numpy().astype(np.float64)
+
+    def state(self) -> dict:
+        """The trained model as plain lists (widths, parameters, feature standardisation)."""
+        return {"widths": list(self.net.widths),
+                "params": self.net.params.cpu().numpy().astype(np.float64).tolist(),
+                "mu": self.mu.cpu().numpy().astype(np.float64).tolist(),
+                "sd": self.sd.cpu().numpy().astype(np.float64).tolist()}
+
+    @classmethod
+    def from_state(cls, st: dict) -> "CostModel":
+        """Rebuilds a trained model from state() (the network lives on the GPU)."""
+        import torch
+        widths = [int(w) for w in st["widths"]]
+        m = cls(widths[0], hidden=widths[1:-1])
+        params = np.asarray(st["params"], dtype=np.float32)
+        if params.size != m.net.n_params:
+            raise ValueError("parameter count does not match the widths")
+        m.net.params.copy_(torch.from_numpy(params))
+        m.mu = torch.as_tensor(np.asarray(st["mu"], dtype=np.float32), device="cuda")
+        m.sd = torch.as_tensor(np.asarray(st["sd"], dtype=np.float32), device="cuda")
+        return m

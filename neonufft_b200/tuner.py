@@ -14,8 +14,9 @@ the reference.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
-from dataclasses import dataclass
+from dataclasses import asdict, dataclass
 
 import numpy as np
 
@@ -232,6 +233,43 @@ class Tuner:
         y = np.array([r[1] for r in rows])
         self.model = CostModel(feats.shape[1], seed=seed)
         return self.model.fit(feats, y, epochs=epochs)
+
+    # ---- persistence: the measured rows and the trained network, versioned -----------------
+    FORMAT = "neonufft_b200.tuner"
+    VERSION = 1
+
+    def save(self, path) -> None:
+        """Writes the sweep's rows (problem, configuration, log10 ms, error) and, when trained,
+        the cost model to a JSON file, so that a tuning run can be reproduced or reused."""
+        doc = {"format": self.FORMAT, "version": self.VERSION, "n_features": N_FEATURES,
+               "rows": [{"problem": asdict(p), "config": {**asdict(c), "tile": list(c.tile)},
+                         "log10_ms": float(lms), "error": float(err)}
+                        for f, lms, err, p, c in self.rows],
+               "model": self.model.state() if self.model is not None else None}
+        with open(path, "w") as fh:
+            json.dump(doc, fh)
+
+    @classmethod
+    def load(cls, path, with_model: bool = True) -> "Tuner":
+        """Reads a file written by save(); the features are recomputed from each row's problem
+        and configuration (host-only). The model needs a GPU; with_model=False skips it."""
+        with open(path) as fh:
+            doc = json.load(fh)
+        if doc.get("format") != cls.FORMAT or int(doc.get("version", 0)) != cls.VERSION:
+            raise ValueError(f"not a version-{cls.VERSION} tuner file: {path}")
+        if int(doc.get("n_features", -1)) != N_FEATURES:
+            raise ValueError("the file's feature set differs from this version's")
+        t = cls()
+        for r in doc["rows"]:
+            p = Problem(**r["problem"])
+            cd = dict(r["config"])
+            cd["tile"] = tuple(int(v) for v in cd["tile"])
+            c = Config(**cd)
+            t.rows.append((features(p, c), float(r["log10_ms"]), float(r["error"]), p, c))
+        if with_model and doc.get("model") is not None:
+            from .costmodel import CostModel
+            t.model = CostModel.from_state(doc["model"])
+        return t
 
     def pick(self, p: Problem, data: ProblemData = None):
         """(configuration, measured (ms, error), candidates tried): the best-ranked candidate

@@ -191,3 +191,29 @@ print("ok")
     res = subprocess.run([sys.executable, "-c", code], cwd=str(ROOT), env=env,
                          capture_output=True, text=True, timeout=120)
     assert res.returncode == 0 and "ok" in res.stdout, res.stdout + res.stderr
+
+
+def test_tuner_rows_round_trip_through_a_file(tmp_path):
+    """The tuner's measured rows (problem, configuration, time, error) survive save / load with
+    their features recomputed identically; a wrong format or version is refused."""
+    from neonufft_b200 import tuner as T
+    t = T.Tuner()
+    probs = [T.Problem(dim=3, type=1, M=10 ** 6, N=64, tol=1e-6, seed=1),
+             T.Problem(dim=2, type=2, M=20000, N=256, tol=1e-3, precision="f32", blob=True, seed=2),
+             T.Problem(dim=3, type=2, M=5 * 10 ** 5, N=48, tol=1e-9, precision="f64", seed=3)]
+    for i, p in enumerate(probs):
+        for j, c in enumerate(T.candidates(p)[:4]):
+            t.rows.append((T.features(p, c), 0.1 * i + 0.01 * j, 1e-7 * (j + 1), p, c))
+    path = tmp_path / "tuner.json"
+    t.save(path)
+    u = T.Tuner.load(path, with_model=False)
+    assert len(u.rows) == len(t.rows)
+    for a, b in zip(t.rows, u.rows):
+        assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+    assert u.autotune(probs[0]) == t.autotune(probs[0])
+    doc = json.loads(path.read_text())
+    doc["version"] = 99
+    bad = tmp_path / "bad.json"
+    bad.write_text(json.dumps(doc))
+    with pytest.raises(ValueError):
+        T.Tuner.load(bad)

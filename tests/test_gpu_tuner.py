@@ -93,3 +93,24 @@ def test_tuner_picks_meet_tol_and_beat_the_rules(cuda, engine):
     if ev["speedup_vs_heuristic_geomean"] is not None:
         assert ev["speedup_vs_heuristic_geomean"] >= MARGIN_VS_HEURISTIC, ev
     assert ev["measurements_per_pick"] <= 0.6 * ev["measurements_exhaustive"], ev
+
+
+def test_trained_tuner_round_trips_through_a_file(tmp_path, cuda, engine):
+    """A trained cost model and its rows saved and loaded again rank candidates identically
+    (the network's parameters and feature standardisation are restored exactly)."""
+    from neonufft_b200 import tuner as T
+    rng = np.random.default_rng(3)
+    t = T.Tuner()
+    for i in range(12):
+        p = T.Problem(dim=2 + i % 2, type=1 + i % 3 // 2, M=int(10 ** rng.uniform(4, 6)),
+                      N=int(rng.choice([32, 64, 128])), tol=float(rng.choice([1e-3, 1e-6])),
+                      seed=i)
+        for c in T.candidates(p):
+            f = T.features(p, c)
+            t.rows.append((f, float(0.1 * f[2] + 0.05 * f[9] + rng.normal(0, 0.01)), 1e-7, p, c))
+    t.train(epochs=300)
+    path = tmp_path / "tuner.json"
+    t.save(path)
+    u = T.Tuner.load(path)
+    feats = np.stack([r[0] for r in t.rows])
+    assert np.array_equal(t.model.predict(feats), u.model.predict(feats))
