@@ -334,6 +334,44 @@ void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* rank
 
 template void launch_bin_count<float>(const BinGeom&, CoordPtrs<float>, i64, u32*, u32*, int*, cudaStream_t);
 template void launch_bin_count<double>(const BinGeom&, CoordPtrs<double>, i64, u32*, u32*, int*, cudaStream_t);
+// Permutation checksum of the bin-sorted records (checked build): sums of perm and perm^2
+// (wrapping 64-bit) into sums[0], sums[1], to compare with those of 0 .. M - 1.
+template <typename T>
+__global__ void __launch_bounds__(kBinBlock)
+    perm_checksum_kernel(const PointRec<T>* rec, i64 M, unsigned long long* sums) {
+  unsigned long long s1 = 0, s2 = 0;
+  for (i64 i = blockIdx.x * i64(kBinBlock) + threadIdx.x; i < M;
+       i += i64(gridDim.x) * kBinBlock) {
+    const unsigned long long p = rec[i].perm;
+    s1 += p;
+    s2 += p * p;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&sums[0], s1);
+    atomicAdd(&sums[1], s2);
+  }
+}
+
+template <typename T>
+void launch_perm_checksum(const PointRec<T>* rec, i64 M, unsigned long long* sums,
+                          cudaStream_t stream) {
+  NNB_CUDA(cudaMemsetAsync(sums, 0, 2 * sizeof(unsigned long long), stream));
+  if (M <= 0) return;
+  i64 grid = (M + kBinBlock - 1) / kBinBlock;
+  if (grid > 148 * 8) grid = 148 * 8;
+  perm_checksum_kernel<T><<<unsigned(grid), kBinBlock, 0, stream>>>(rec, M, sums);
+  NNB_LAUNCH_CHECK();
+}
+template void launch_perm_checksum<float>(const PointRec<float>*, i64, unsigned long long*,
+                                          cudaStream_t);
+template void launch_perm_checksum<double>(const PointRec<double>*, i64, unsigned long long*,
+                                           cudaStream_t);
+
 template void launch_bin_scatter<float>(const BinGeom&, CoordPtrs<float>, i64, const u32*, const u32*, PointRec<float>*, cudaStream_t);
 template void launch_bin_scatter<double>(const BinGeom&, CoordPtrs<double>, i64, const u32*, const u32*, PointRec<double>*, cudaStream_t);
 

@@ -21,6 +21,9 @@ i64 scan_tmp_words(i64 n);
 void launch_exclusive_scan(const u32* counts, u32* out, i64 n, u32* tmp, cudaStream_t stream);
 // Pass 2: one 32-byte record per point (permutation, packed cell, fractions) in tile order.
 template <typename T>
+void launch_perm_checksum(const PointRec<T>* rec, i64 M, unsigned long long* sums,
+                          cudaStream_t stream);
+template <typename T>
 void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* ranks,
                         const u32* bin_start, PointRec<T>* rec, cudaStream_t stream);
 

@@ -270,11 +270,29 @@ void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t st
   launch_bin_scatter<T>(g, x, M, ranks_.data(), bin_start_.data(), rec_.data(), stream);
   int host_err = 0;
   NNB_CUDA(cudaMemcpyAsync(&host_err, err_.data(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+#ifdef NNB_CHECKED
+  // The records' permutation must be 0 .. M - 1, each once: compare its sum and sum of squares
+  // (wrapping 64-bit, as the device adds them) with the closed forms.
+  checksum_.reserve(2);
+  unsigned long long sums[2] = {0, 0};
+  launch_perm_checksum<T>(rec_.data(), M, checksum_.data(), stream);
+  NNB_CUDA(cudaMemcpyAsync(sums, checksum_.data(), sizeof(sums), cudaMemcpyDeviceToHost, stream));
+#endif
   NNB_CUDA(cudaStreamSynchronize(stream));
   if (host_err) {
     M_ = 0;
     throw_input("non-finite point coordinate");
   }
+#ifdef NNB_CHECKED
+  const unsigned __int128 m = static_cast<unsigned __int128>(M);
+  const unsigned long long want1 = static_cast<unsigned long long>(m * (m - (M > 0)) / 2);
+  const unsigned long long want2 =
+      M > 0 ? static_cast<unsigned long long>((m - 1) * m * (2 * m - 1) / 6) : 0ull;
+  if (sums[0] != want1 || sums[1] != want2) {
+    M_ = 0;
+    throw_internal("checked build: the bin-sorted records are not a permutation of the points");
+  }
+#endif
 }
 
 template <typename T>

@@ -147,7 +147,8 @@ class PointSet {
 public:
   explicit PointSet(std::shared_ptr<DeviceAllocator> alloc);
   // Bins M points; enqueues work on `stream`, then synchronises it and throws InputError for
-  // non-finite coordinates.
+  // non-finite coordinates (and, in the checked build, InternalError when the records' point
+  // indices are not a permutation of 0 .. M - 1).
   void build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream);
   SortedPoints<T> view() const;
   i64 size() const { return M_; }
@@ -159,6 +160,7 @@ private:
   DevArray<PointRec<T>> rec_;
   DevArray<u32> counts_, bin_start_, ranks_, scan_tmp_, work_start_, work_owner_;
   DevArray<int> err_;
+  DevArray<unsigned long long> checksum_;  // checked build: permutation checksum of the records
 };
 
 // Spreading / interpolation method for a plan: the requested one (validated), or the default:
