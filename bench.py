@@ -853,9 +853,9 @@ def run_transform(args, wl):
     h2d = dim * M * rsz + (M * csz if 1 in types else 0) + (nm * csz if 2 in types else 0)
     d2h = (nm * csz if 1 in types else 0) + (M * csz if 2 in types else 0)
 
-    # Pipelined as a caller would run a stream of transforms: two device buffer sets; step i's
-    # host->device copies run on an upload stream while step i-1 computes, and step i-1's
-    # device->host copies on a download stream while step i computes. Events order every reuse
+    # Pipelined as a caller would run a stream of transforms: two device buffer sets; step i+1's
+    # host->device copies run on an upload stream while step i computes, and step i's
+    # device->host copies on a download stream while step i+1 computes. Events order every reuse
     # of a buffer set; every step still moves all of its inputs and outputs.
     comp = torch.cuda.current_stream()
     up, down = torch.cuda.Stream(), torch.cuda.Stream()
@@ -870,7 +870,7 @@ def run_transform(args, wl):
     for ev in computed + downloaded:
         ev.record(comp)
 
-    def e2e_step(i):
+    def upload(i):
         j = i % 2
         b = bufs[j]
         up.wait_event(computed[j])  # the compute that last read this buffer set is done
@@ -882,6 +882,10 @@ def run_transform(args, wl):
             if 2 in types:
                 b["f"].copy_(f_h, non_blocking=True)
         uploaded[j].record(up)
+
+    def compute_and_download(i):
+        j = i % 2
+        b = bufs[j]
         comp.wait_event(uploaded[j])
         comp.wait_event(downloaded[j])  # the last download of these outputs is done
         step(b["loc"], b["f"], b["c"], b["o2"], b["o1"])
@@ -894,14 +898,21 @@ def run_transform(args, wl):
                 o2_h.copy_(b["o2"], non_blocking=True)
         downloaded[j].record(down)
 
-    for i in range(2):
-        e2e_step(i)
+    # set_points synchronises its stream once the points are binned (as the reference's does),
+    # so the next step's uploads are enqueued before this step's set_points blocks the host.
+    def run_steps(n):
+        upload(0)
+        for i in range(n):
+            if i + 1 < n:
+                upload(i + 1)
+            compute_and_download(i)
+
+    run_steps(2)
     torch.cuda.synchronize()
     barrier()
     e0.record(comp)
     up.wait_stream(comp)
-    for i in range(args.steps):
-        e2e_step(i)
+    run_steps(args.steps)
     comp.wait_stream(down)
     e1.record(comp)
     torch.cuda.synchronize()

@@ -242,7 +242,7 @@ template class FftGrid<double>;
 template <typename T>
 PointSet<T>::PointSet(std::shared_ptr<DeviceAllocator> alloc)
     : rec_(alloc), counts_(alloc), bin_start_(alloc), ranks_(alloc), scan_tmp_(alloc),
-      work_start_(alloc), work_owner_(alloc), err_(alloc) {}
+      work_start_(alloc), work_owner_(alloc), err_(alloc), checksum_(alloc) {}
 
 template <typename T>
 void PointSet<T>::build(const BinGeom& g, CoordPtrs<T> x, i64 M, cudaStream_t stream) {

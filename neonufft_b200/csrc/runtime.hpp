@@ -51,6 +51,7 @@ public:
       return;
     }
     release();
+    if (n && !alloc_) throw_internal("device array without an allocator");
     if (n) ptr_ = static_cast<X*>(alloc_->allocate(n * sizeof(X)));
     cap_ = n;
     n_ = n;
