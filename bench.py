@@ -740,6 +740,38 @@ def reference_gpu_arm(torch, wl, args, loc, c, f, refs, barrier):
             "source": "reference GPU plan built from its own sources (oracle/_ref)"}
 
 
+def reuse_arm(nnb, torch, wl, args, loc, c, opt, refs, barrier, nvec=8):
+    """Point-set reuse (the plan API's separate set_points): one set_points, then
+    `nvec` type-1 transforms of different strength vectors on the same points, with the tuned
+    options. Reported beside the single-transform line, as NU points per second per transform;
+    the first vector is the line's own strengths, checked against the same direct sums."""
+    dim, M, N = wl["dim"], wl["M"], wl["N"]
+    nm = N ** dim
+    strides = [1, N, N * N][:dim]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4321)
+    vecs = [c] + [torch.complex(torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype),
+                                torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype))
+                  for _ in range(nvec - 1)]
+    outs = [torch.empty(nm, dtype=c.dtype, device="cuda") for _ in range(nvec)]
+    plan = nnb.Plan(opt, -1, M, loc, [N] * dim)
+
+    def step():
+        plan.set_points(M, loc)
+        for v, o in zip(vecs, outs):
+            plan.transform_type_1(v, o, strides)
+
+    ms = timed_steps(torch, step, args.steps, args.warmup, barrier)
+    acc = arm_accuracy(torch, {1: refs[1]}, {1: outs[0]}) if refs and 1 in refs else {}
+    plan.close()
+    del vecs, outs
+    torch.cuda.empty_cache()
+    return {"transforms_per_set_points": nvec, "ms_per_step": ms,
+            "points_per_s_per_transform": nvec * M / (ms * 1e-3), "steps": args.steps,
+            "accuracy_first_vector": acc,
+            "step": f"set_points + {nvec} x transform_type_1 (same points, {nvec} strength vectors)"}
+
+
 def run_transform(args, wl):
     """Single-transform workloads (ns, c2, c1): the tuned engine arm (the line's value and e2e),
     then the plain FP64 arm and the reference's FP64 GPU plan on the same inputs."""
@@ -935,10 +967,12 @@ def run_transform(args, wl):
         acc["meets_tol"] = all(v <= tol for k, v in acc.items() if k.endswith("rel_l2"))
 
     # ---- the plain FP64 GPU path and the reference's FP64 GPU plan (same inputs) ------------
-    plain = ref_gpu = None
+    plain = ref_gpu = reuse = None
     if not args.no_extra_arms:
         plain = plain_fp64_arm(nnb, torch, wl, args, loc, c, f, refs, barrier)
         ref_gpu = reference_gpu_arm(torch, wl, args, loc, c, f, refs, barrier)
+        if types == (1,):
+            reuse = reuse_arm(nnb, torch, wl, args, loc, c, opt, refs, barrier)
 
     # ---- roofline of the dominant kernel -----------------------------------------------------
     peak, peak_kind = load_peaks()
@@ -1021,6 +1055,9 @@ def run_transform(args, wl):
             "reference_gpu_fp64": ref_gpu,
             "ratio_vs_reference_gpu_fp64": (value / ref_gpu["points_per_s"])
             if ref_gpu and "points_per_s" in ref_gpu else None,
+            "point_set_reuse": reuse,
+            "reuse_ratio_vs_plain_fp64": (reuse["points_per_s_per_transform"] /
+                                          plain["points_per_s"]) if reuse and plain else None,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
