@@ -57,8 +57,9 @@ typedef struct NnbOptions {
   int order;                /* NeonufftModeOrder */
   int kernel_type;          /* NeonufftKernelType */
   int tile[3];              /* subproblem tile (bin) shape in fine-grid cells; 0 = automatic.
-                               Method 3 takes {2|4|8, 8|16, 1} (16 rows: single precision);
-                               the default is {4, 8, 1} */
+                               Method 3 takes {2|4|8, 8|16, 1} (16 rows: single precision) and
+                               {4, 4, 1} (single precision); the default is {4, 8, 1}.
+                               Method 5 uses {4, 4, 1} */
   int spread_method;        /* 0 = automatic (3 for 3D plans with kernel width <= 8, else 1);
                                1 = warp-private shared-memory slabs; 2 = thread per point;
                                3 = sliding z-window held in registers (3D, width <= 8);
