@@ -742,7 +742,8 @@ def reference_gpu_arm(torch, wl, args, loc, c, f, refs, barrier):
 
 def reuse_arm(nnb, torch, wl, args, loc, c, opt, refs, barrier, nvec=8):
     """Point-set reuse (the plan API's separate set_points): one set_points, then
-    `nvec` type-1 transforms of different strength vectors on the same points, with the tuned
+    `nvec` type-1 transforms of different strength vectors on the same points
+    (transform_type_1_many: single precision spreads two vectors per pass), with the tuned
     options. Reported beside the single-transform line, as NU points per second per transform;
     the first vector is the line's own strengths, checked against the same direct sums."""
     dim, M, N = wl["dim"], wl["M"], wl["N"]
@@ -750,26 +751,28 @@ def reuse_arm(nnb, torch, wl, args, loc, c, opt, refs, barrier, nvec=8):
     strides = [1, N, N * N][:dim]
     g = torch.Generator(device="cuda")
     g.manual_seed(4321)
-    vecs = [c] + [torch.complex(torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype),
-                                torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype))
-                  for _ in range(nvec - 1)]
-    outs = [torch.empty(nm, dtype=c.dtype, device="cuda") for _ in range(nvec)]
+    vecs = torch.empty(nvec * M, dtype=c.dtype, device="cuda")
+    vecs[:M] = c
+    for v in range(1, nvec):
+        vecs[v * M:(v + 1) * M] = torch.complex(
+            torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype),
+            torch.randn(M, generator=g, device="cuda", dtype=c.real.dtype))
+    outs = torch.empty(nvec * nm, dtype=c.dtype, device="cuda")
     plan = nnb.Plan(opt, -1, M, loc, [N] * dim)
 
     def step():
         plan.set_points(M, loc)
-        for v, o in zip(vecs, outs):
-            plan.transform_type_1(v, o, strides)
+        plan.transform_type_1_many(vecs, outs, nvec, strides)
 
     ms = timed_steps(torch, step, args.steps, args.warmup, barrier)
-    acc = arm_accuracy(torch, {1: refs[1]}, {1: outs[0]}) if refs and 1 in refs else {}
+    acc = arm_accuracy(torch, {1: refs[1]}, {1: outs[:nm]}) if refs and 1 in refs else {}
     plan.close()
     del vecs, outs
     torch.cuda.empty_cache()
     return {"transforms_per_set_points": nvec, "ms_per_step": ms,
             "points_per_s_per_transform": nvec * M / (ms * 1e-3), "steps": args.steps,
             "accuracy_first_vector": acc,
-            "step": f"set_points + {nvec} x transform_type_1 (same points, {nvec} strength vectors)"}
+            "step": f"set_points + transform_type_1_many of {nvec} strength vectors"}
 
 
 def run_transform(args, wl):

@@ -114,6 +114,18 @@ NNB_API NeonufftError nnb_plan_set_points(NnbPlan plan, int64_t num_nu, const vo
 NNB_API NeonufftError nnb_plan_transform_type_1(NnbPlan plan, const void* in, void* out,
                                         const int64_t* out_strides);
 
+/* `count` type-1 transforms of the plan's points (engine extension; the reference's type-1/2
+ * plan transforms one vector per call): strength vector v at in + v * in_bdist, its modes at
+ * out + v * out_bdist (elements; out_bdist at least the span of the strided mode box). Single
+ * precision on the z-window kernels (spread methods 3 with the default or 4-row tiles) spreads
+ * the vectors two at a time, each staged point serving both, and holds two extra fine grids for
+ * it; other plans run the transforms one at a time. Same results as `count` calls of
+ * nnb_plan_transform_type_1. */
+NNB_API NeonufftError nnb_plan_transform_type_1_many(NnbPlan plan, int64_t count, const void* in,
+                                                     int64_t in_bdist, void* out,
+                                                     int64_t out_bdist,
+                                                     const int64_t* out_strides);
+
 /* Type 2: out[j] = sum_k in[k] exp(i*sign*k.x_j), in read with in_strides (in elements).
  * Replaces gpu::Plan<T,DIM>::transform_type_2 (reference include/neonufft/gpu/plan.hpp:37-39). */
 NNB_API NeonufftError nnb_plan_transform_type_2(NnbPlan plan, const void* in, const int64_t* in_strides,

@@ -63,6 +63,7 @@ SIGNATURES = [
     ("nnb_plan_set_points", _E, [_P, _I64, _PP]),
     ("nnb_plan_transform_type_1", _E, [_P, _P, _P, _PI64]),
     ("nnb_plan_transform_type_2", _E, [_P, _P, _PI64, _P]),
+    ("nnb_plan_transform_type_1_many", _E, [_P, _I64, _P, _I64, _P, _I64, _PI64]),
     ("nnb_plan_destroy", _E, [_P]),
     ("nnb_plan_t3_grid_memory_size", _E, [C.c_int, C.c_int, C.POINTER(NnbOptions), _PD, _PD, _PD, _PD, C.POINTER(C.c_uint64)]),
     ("nnb_plan_t3_create", _E, [C.POINTER(_P), C.c_int, C.c_int, C.POINTER(NnbOptions), C.c_int, _I64, _PP, _I64, _PP, _P, _I64, C.POINTER(NnbAllocator)]),

@@ -251,6 +251,15 @@ NeonufftError nnb_plan_transform_type_1(NnbPlan plan, const void* in, void* out,
   });
 }
 
+NeonufftError nnb_plan_transform_type_1_many(NnbPlan plan, int64_t count, const void* in,
+                                             int64_t in_bdist, void* out, int64_t out_bdist,
+                                             const int64_t* out_strides) {
+  return guard([&] {
+    need(plan, "plan");
+    plan->impl->transform_type_1_many(count, in, in_bdist, out, out_bdist, out_strides);
+  });
+}
+
 NeonufftError nnb_plan_transform_type_2(NnbPlan plan, const void* in, const int64_t* in_strides,
                                         void* out) {
   return guard([&] {

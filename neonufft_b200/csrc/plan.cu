@@ -1,4 +1,5 @@
 // Plan implementations (see plan.hpp).
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 #include <vector>
@@ -45,6 +46,17 @@ void check_strides(int dim, const i64* modes, const i64* strides) {
 
 }  // namespace
 
+void PlanBase::transform_type_1_many(i64 count, const void* in, i64 in_bdist, void* out,
+                                     i64 out_bdist, const i64* out_strides) {
+  NnbPlanInfo inf{};
+  info(&inf);
+  const size_t csz = inf.precision == NNB_FLOAT ? 8 : 16;
+  for (i64 v = 0; v < count; ++v) {
+    transform_type_1(static_cast<const char*>(in) + size_t(v * in_bdist) * csz,
+                     static_cast<char*>(out) + size_t(v * out_bdist) * csz, out_strides);
+  }
+}
+
 void PlanBase::fused_job(int, const void*, void*, void*) const {
   throw_internal("plan has no persistent z-window step");
 }
@@ -87,7 +99,8 @@ public:
         opt_(opt),
         sign_(sign < 0 ? -1 : 1),
         stream_(stream),
-        points_(alloc_) {
+        points_(alloc_),
+        pair_grid_(alloc_) {
     if (!modes) throw_input("null modes");
     for (int d = 0; d < 3; ++d) {
       modes_[d] = 1;
@@ -136,6 +149,57 @@ public:
       ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
       launch_downsample<T>(deconv_args(out_strides), fft_->data(), static_cast<cplx_t<T>*>(out),
                            stream_);
+    }
+  }
+
+  // Single precision on the z-window kernels (default or 4-row tiles) spreads the vectors two
+  // at a time: each staged point serves both, into a pair of fine grids; each grid is then
+  // transformed and deconvolved into its output.
+  void transform_type_1_many(i64 count, const void* in, i64 in_bdist, void* out, i64 out_bdist,
+                             const i64* out_strides) override {
+    const i64 M = points_.size();
+    if (count < 0) throw_input("negative number of transforms");
+    if (count == 0) return;
+    if (!out) throw_input("null output");
+    if (M > 0 && !in) throw_input("null input");
+    check_strides(dim_, modes_, out_strides);
+    i64 extent = 1;
+    for (int d = 0; d < dim_; ++d) extent += (modes_[d] - 1) * out_strides[d];
+    if (count > 1 && (in_bdist < M || out_bdist < extent)) {
+      throw_input("input / output distances smaller than one vector");
+    }
+    const bool pairs = is_single<T>() && method_ == 3 && tile_[0] == 4 &&
+                       (tile_[1] == 8 || tile_[1] == 4) && count > 1 && M > 0;
+    if (!pairs) {
+      PlanBase::transform_type_1_many(count, in, in_bdist, out, out_bdist, out_strides);
+      return;
+    }
+    const auto* iv = static_cast<const cplx_t<T>*>(in);
+    auto* ov = static_cast<cplx_t<T>*>(out);
+    const i64 cells = fft_->cells();
+    pair_grid_.reserve(size_t(2 * cells));
+    for (i64 v = 0; v < count; v += 2) {
+      const i64 nv = std::min<i64>(2, count - v);
+      NNB_CUDA(cudaMemsetAsync(pair_grid_.data(), 0, sizeof(cplx_t<T>) * size_t(nv * cells),
+                               stream_));
+      {
+        ScopedStage st(timer_, stream_, NNB_STAGE_SPREAD);
+        SpreadArgs<T> a = spread_args(iv + v * in_bdist);
+        a.grid = pair_grid_.data();
+        a.in_bdist = in_bdist;
+        a.grid_bdist = cells;
+        a.batch = int(nv);
+        launch_spread<T>(a, stream_);
+      }
+      for (i64 j = 0; j < nv; ++j) {
+        cplx_t<T>* gj = pair_grid_.data() + j * cells;
+        {
+          ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
+          fft_->exec_on(gj, stream_);
+        }
+        ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
+        launch_downsample<T>(deconv_args(out_strides), gj, ov + (v + j) * out_bdist, stream_);
+      }
     }
   }
 
@@ -273,6 +337,7 @@ private:
   std::unique_ptr<FftGrid<T>> fft_;
   DevArray<T> corr_[3];
   PointSet<T> points_;
+  DevArray<cplx_t<T>> pair_grid_;  // two fine grids for transform_type_1_many
   StageTimer timer_;
 };
 

@@ -18,6 +18,10 @@ public:
   virtual void set_points(i64 M, const void* const* loc) = 0;
   virtual void transform_type_1(const void* in, void* out, const i64* out_strides) = 0;
   virtual void transform_type_2(const void* in, const i64* in_strides, void* out) = 0;
+  // `count` type-1 transforms of the plan's points: input vector v at in + v in_bdist, output
+  // v at out + v out_bdist (elements). The base runs them one at a time.
+  virtual void transform_type_1_many(i64 count, const void* in, i64 in_bdist, void* out,
+                                     i64 out_bdist, const i64* out_strides);
   virtual void info(NnbPlanInfo* info) const = 0;
   virtual StageTimer& timer() = 0;
   virtual cudaStream_t stream() const = 0;

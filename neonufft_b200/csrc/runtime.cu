@@ -223,15 +223,18 @@ FftGrid<T>::~FftGrid() {
 }
 
 template <typename T>
-void FftGrid<T>::exec(cudaStream_t stream) {
+void FftGrid<T>::exec(cudaStream_t stream) { exec_on(grid_.data(), stream); }
+
+template <typename T>
+void FftGrid<T>::exec_on(cplx_t<T>* data, cudaStream_t stream) {
   NNB_CUFFT(cufftSetStream(plan_, stream));
   const int dir = sign_ < 0 ? CUFFT_FORWARD : CUFFT_INVERSE;
   if constexpr (std::is_same<T, float>::value) {
-    NNB_CUFFT(cufftExecC2C(plan_, reinterpret_cast<cufftComplex*>(grid_.data()),
-                           reinterpret_cast<cufftComplex*>(grid_.data()), dir));
+    NNB_CUFFT(cufftExecC2C(plan_, reinterpret_cast<cufftComplex*>(data),
+                           reinterpret_cast<cufftComplex*>(data), dir));
   } else {
-    NNB_CUFFT(cufftExecZ2Z(plan_, reinterpret_cast<cufftDoubleComplex*>(grid_.data()),
-                           reinterpret_cast<cufftDoubleComplex*>(grid_.data()), dir));
+    NNB_CUFFT(cufftExecZ2Z(plan_, reinterpret_cast<cufftDoubleComplex*>(data),
+                           reinterpret_cast<cufftDoubleComplex*>(data), dir));
   }
 }
 

@@ -127,6 +127,9 @@ public:
           cudaStream_t stream);
   ~FftGrid();
   void exec(cudaStream_t stream);
+  // The same in-place transform on another buffer of the grid's shape (the plan's work area is
+  // shared: executions on one stream are ordered).
+  void exec_on(cplx_t<T>* data, cudaStream_t stream);
   cplx_t<T>* data() const { return grid_.data(); }
   i64 cells() const { return cells_; }
   const i64* nf() const { return nf_; }

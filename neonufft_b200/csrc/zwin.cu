@@ -310,16 +310,23 @@ struct ZThread {
 };
 
 // ---- spreading ---------------------------------------------------------------------------------
-template <typename T, int W, int TX, int TY = 8>
+// NV strength vectors on the same points (NV = 2: the second vector's staged strengths).
+template <typename T, int W, int TX, int TY = 8, int NV = 1>
 struct ZSpreadShared {
   ZSlot<T, W, TX, TY> slots[2][ZShape<T, W, TX, TY>::BATCH];
+  cplx_t<T> v2[2][NV > 1 ? ZShape<T, W, TX, TY>::BATCH : 1];
 };
 
-// Spreads work item `item` of batch entry `batch` (one CTA; every thread calls it).
-template <typename T, int W, int TX, int TY = 8>
+// Spreads work item `item` of batch entries batch .. batch + NV - 1 (one CTA; every thread
+// calls it). With NV = 2 each staged point, its kernel values and the window's bookkeeping
+// serve two strength vectors on the same points (type-3 batches, repeated type-1 transforms):
+// the second vector's row sums sit in their own registers and go to the next grid (at
+// grid_bdist); a missing second entry (an odd batch) is skipped.
+template <typename T, int W, int TX, int TY = 8, int NV = 1>
 __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks ch,
                                                  const WorkList& wl, u32 item, int batch,
-                                                 ZSpreadShared<T, W, TX, TY>& sh) {
+                                                 ZSpreadShared<T, W, TX, TY, NV>& sh) {
+  static_assert(NV == 1 || NV == 2, "one or two strength vectors per pass");
   using S = ZShape<T, W, TX, TY>;
   using Ops = Packed<T>;
   using P = typename Ops::P;
@@ -333,6 +340,7 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
   const ZThread<T, W, TX, TY> th;
   const C* in = a.in + batch * a.in_bdist;
   C* grid = a.grid + batch * a.grid_bdist;
+  const bool has2 = NV > 1 && batch + 1 < a.batch;  // the second vector exists
   const i64 nfx = g.nf[0], nfy = g.nf[1], nfz = g.nf[2];
   [[maybe_unused]] const i64 cells = nfx * nfy * nfz;
   const bool narrow = nfx < S::P0;
@@ -340,47 +348,59 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
   const i64 row_y = has_row ? wrap_add(i64(cta.ty) * S::TY, th.ra, nfy) : 0;
   const i64 gx0 = i64(cta.tx) * TX;
 
-  P are[S::NP], aim[S::NP];  // real / imaginary parts of cell pairs (2q, 2q + 1) of the row
+  // real / imaginary parts of cell pairs (2q, 2q + 1) of the row, per strength vector
+  P are[NV][S::NP], aim[NV][S::NP];
 #pragma unroll
-  for (int q = 0; q < S::NP; ++q) are[q] = aim[q] = Ops::zero();
+  for (int v = 0; v < NV; ++v) {
+#pragma unroll
+    for (int q = 0; q < S::NP; ++q) are[v][q] = aim[v][q] = Ops::zero();
+  }
   bool dirty = false;
 
-  // Adds this thread's row of plane p (absolute; may exceed nfz) to the grid and clears it.
+  // Adds this thread's row of plane p (absolute; may exceed nfz) to the grid(s) and clears it.
   // The region's x range lies inside the grid and its rows start 16-byte aligned (the usual
   // case): whole cell pairs are added with one vector atomic each.
   const bool pairs = !narrow && gx0 + S::P0 <= nfx && (nfx % 2) == 0 &&
-                     (reinterpret_cast<size_t>(grid) % 16) == 0;
+                     (reinterpret_cast<size_t>(grid) % 16) == 0 &&
+                     (NV == 1 || (a.grid_bdist % 2) == 0);
   auto flush = [&](int p) {
     if (has_row && dirty) {
       const i64 base = (wrap_plane(p, nfz) * nfy + row_y) * nfx;
-      C* row = grid + base;
-      if (pairs) {
-        C* r = row + gx0;
 #pragma unroll
-        for (int q = 0; q < S::NP; ++q) {
-          if (2 * q + 1 < S::P0) {
-            if (NNB_CHECK_INDEX(base + gx0 + 2 * q + 1, cells)) {
-              atomic_add_pair(r + 2 * q, Ops::lo(are[q]), Ops::lo(aim[q]), Ops::hi(are[q]),
-                              Ops::hi(aim[q]));
+      for (int v = 0; v < NV; ++v) {
+        if (v == 1 && !has2) break;
+        C* row = grid + v * a.grid_bdist + base;
+        if (pairs) {
+          C* r = row + gx0;
+#pragma unroll
+          for (int q = 0; q < S::NP; ++q) {
+            if (2 * q + 1 < S::P0) {
+              if (NNB_CHECK_INDEX(base + gx0 + 2 * q + 1, cells)) {
+                atomic_add_pair(r + 2 * q, Ops::lo(are[v][q]), Ops::lo(aim[v][q]),
+                                Ops::hi(are[v][q]), Ops::hi(aim[v][q]));
+              }
+            } else if (NNB_CHECK_INDEX(base + gx0 + 2 * q, cells)) {
+              atomic_add_cplx(r + 2 * q, C{Ops::lo(are[v][q]), Ops::lo(aim[v][q])});
             }
-          } else if (NNB_CHECK_INDEX(base + gx0 + 2 * q, cells)) {
-            atomic_add_cplx(r + 2 * q, C{Ops::lo(are[q]), Ops::lo(aim[q])});
           }
-          are[q] = aim[q] = Ops::zero();
-        }
-      } else {
+        } else {
 #pragma unroll
-        for (int q = 0; q < S::NP; ++q) {
-          const i64 x0 = wrap_x(gx0, 2 * q, nfx, narrow);
-          if (NNB_CHECK_INDEX(base + x0, cells)) {
-            atomic_add_cplx(&row[x0], C{Ops::lo(are[q]), Ops::lo(aim[q])});
+          for (int q = 0; q < S::NP; ++q) {
+            const i64 x0 = wrap_x(gx0, 2 * q, nfx, narrow);
+            if (NNB_CHECK_INDEX(base + x0, cells)) {
+              atomic_add_cplx(&row[x0], C{Ops::lo(are[v][q]), Ops::lo(aim[v][q])});
+            }
+            const i64 x1 = wrap_x(gx0, 2 * q + 1, nfx, narrow);
+            if (2 * q + 1 < S::P0 && NNB_CHECK_INDEX(base + x1, cells)) {
+              atomic_add_cplx(&row[x1], C{Ops::hi(are[v][q]), Ops::hi(aim[v][q])});
+            }
           }
-          const i64 x1 = wrap_x(gx0, 2 * q + 1, nfx, narrow);
-          if (2 * q + 1 < S::P0 && NNB_CHECK_INDEX(base + x1, cells)) {
-            atomic_add_cplx(&row[x1], C{Ops::hi(are[q]), Ops::hi(aim[q])});
-          }
-          are[q] = aim[q] = Ops::zero();
         }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+#pragma unroll
+        for (int q = 0; q < S::NP; ++q) are[v][q] = aim[v][q] = Ops::zero();
       }
     }
     dirty = false;
@@ -403,6 +423,19 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
                                  min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane,
                                  a.pts.M);
     }
+    if constexpr (NV > 1) {  // the second vector's strengths at the staged points
+      __syncwarp();
+      if (th.lane < count) {
+        const int j = th.warp * PW + th.lane;
+        C v2{T(0), T(0)};
+        const u32 perm = slots[k & 1][j].perm;
+        if (has2 && NNB_CHECK_INDEX(perm, a.pts.M)) {
+          v2 = in[a.in_bdist + perm];
+          if (a.prephase) v2 = cmul(v2, a.prephase[perm]);
+        }
+        sh.v2[k & 1][j] = v2;
+      }
+    }
   };
 
   stage(0);
@@ -423,7 +456,8 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
 #pragma unroll
     for (int h = 0; h < (S::BATCH + 31) / 32; ++h) {
       for (u32 m = own[h]; m != 0u; m &= m - 1u) {
-        const Slot& sl = sb[h * 32 + __ffs(int(m)) - 1];
+        const int si = h * 32 + __ffs(int(m)) - 1;
+        const Slot& sl = sb[si];
         const int tp = sl.lyp >> 4;
         if (tp != cur) {  // advance the window: planes [cur, tp) are complete
           const int n = min(tp - cur, S::RZ);
@@ -435,9 +469,17 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
         }
         dirty = true;
         const T kw = sl.ky[th.ra] * sl.kz[dz];
-        const C v = sl.v;
-        const P wre = Ops::splat(v.x * kw);
-        const P wim = Ops::splat(v.y * kw);
+        P wre[NV], wim[NV];
+        {
+          const C v = sl.v;
+          wre[0] = Ops::splat(v.x * kw);
+          wim[0] = Ops::splat(v.y * kw);
+        }
+        if constexpr (NV > 1) {
+          const C v = sh.v2[k & 1][si];
+          wre[1] = Ops::splat(v.x * kw);
+          wim[1] = Ops::splat(v.y * kw);
+        }
 #pragma unroll
         for (int q = 0; q < S::NP; q += 2) {
           P kk[2];
@@ -445,8 +487,11 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             if (q + u < S::NP) {
-              are[q + u] = Ops::fma(kk[u], wre, are[q + u]);
-              aim[q + u] = Ops::fma(kk[u], wim, aim[q + u]);
+#pragma unroll
+              for (int v = 0; v < NV; ++v) {
+                are[v][q + u] = Ops::fma(kk[u], wre[v], are[v][q + u]);
+                aim[v][q + u] = Ops::fma(kk[u], wim[v], aim[v][q + u]);
+              }
             }
           }
         }
@@ -464,6 +509,15 @@ __global__ void __launch_bounds__(ZShape<T, W, TX, TY>::NT)
                        const __grid_constant__ WorkList wl) {
   __shared__ ZSpreadShared<T, W, TX, TY> sh;
   spread_zwin_item<T, W, TX, TY>(a, ch, wl, blockIdx.x, int(blockIdx.y), sh);
+}
+
+// Two strength vectors per CTA: batch entries 2 blockIdx.y and 2 blockIdx.y + 1.
+template <typename T, int W, int TX, int TY>
+__global__ void __launch_bounds__(ZShape<T, W, TX, TY>::NT)
+    spread_zwin2_kernel(const __grid_constant__ SpreadArgs<T> a, ZChunks ch,
+                        const __grid_constant__ WorkList wl) {
+  __shared__ ZSpreadShared<T, W, TX, TY, 2> sh;
+  spread_zwin_item<T, W, TX, TY, 2>(a, ch, wl, blockIdx.x, 2 * int(blockIdx.y), sh);
 }
 
 // Takes the next item of the queue spanning all jobs; every thread returns the same values.
@@ -991,6 +1045,17 @@ void launch_spread_zwin_tw(const SpreadArgs<T>& a, cudaStream_t stream) {
   const i64 ncols = i64(a.g.ntiles[0]) * a.g.ntiles[1];
   const ZChunks ch = make_chunks(ncols, a.g.ntiles[2], W);
   const WorkList wl = zwin_work_list(a.g, a.pts, ch, stream);
+  // Single precision with the default or 4-row tiles spreads two strength vectors per pass
+  // when there are several (the second vector costs its FMAs only).
+  constexpr bool kPairs = std::is_same<T, float>::value && TX == 4 && (TY == 8 || TY == 4);
+  if constexpr (kPairs) {
+    if (a.batch > 1) {
+      dim3 grid{unsigned(wl.grid), unsigned((a.batch + 1) / 2), 1u};
+      spread_zwin2_kernel<T, W, TX, TY><<<grid, S::NT, 0, stream>>>(a, ch, wl);
+      NNB_LAUNCH_CHECK();
+      return;
+    }
+  }
   dim3 grid{unsigned(wl.grid), unsigned(a.batch), 1u};
   spread_zwin_kernel<T, W, TX, TY><<<grid, S::NT, 0, stream>>>(a, ch, wl);
   NNB_LAUNCH_CHECK();

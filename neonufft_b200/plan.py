@@ -171,6 +171,7 @@ class Plan:
             raise InputError("loc and modes must have the same length")
         self.precision = _precision(dtype, loc)
         self.modes = [int(m) for m in modes]
+        self.num_nu = int(num_nu)
         self._stream = _stream(stream)
         self._alloc = _Alloc(device_alloc) if device_alloc is not None else None
         h = C.c_void_p()
@@ -185,11 +186,27 @@ class Plan:
         check(L.load().nnb_plan_transform_type_1(self._h, _ptr(inp), _ptr(out),
                                                  L.i64_array(out_strides)))
 
+    def transform_type_1_many(self, inp, out, count: int, out_strides: Sequence[int],
+                              in_bdist: int = 0, out_bdist: int = 0) -> None:
+        """`count` type-1 transforms of the plan's points (engine extension): vector v of `inp`
+        at offset v * in_bdist (default: the number of points), its modes at v * out_bdist of
+        `out` (default: the number of modes). Single-precision plans on the z-window kernels
+        spread two vectors per pass."""
+        nm = 1
+        for m in self.modes:
+            nm *= int(m)
+        in_bdist = int(in_bdist) or int(self.num_nu)
+        out_bdist = int(out_bdist) or nm
+        check(L.load().nnb_plan_transform_type_1_many(self._h, int(count), _ptr(inp), in_bdist,
+                                                      _ptr(out), out_bdist,
+                                                      L.i64_array(out_strides)))
+
     def transform_type_2(self, inp, in_strides: Sequence[int], out) -> None:
         check(L.load().nnb_plan_transform_type_2(self._h, _ptr(inp), L.i64_array(in_strides),
                                                  _ptr(out)))
 
     def set_points(self, num_nu: int, loc: Sequence) -> None:
+        self.num_nu = int(num_nu)
         check(L.load().nnb_plan_set_points(self._h, int(num_nu),
                                            L.ptr_array([_ptr(a) for a in loc])))
 
