@@ -49,7 +49,10 @@ def test_tcgen05_spreading_matches_zwin_and_direct(w, case, cuda, engine, oracle
     assert info5["spread_method"] == 5 and list(info5["tile"]) == [4, 4, 1]
     ref = direct(oracle, 1, -1, pts, c, modes, "float32")
     assert oracle.rel_l2(out5, ref) < width_bound("float32", w)
-    assert oracle.rel_l2(out5, out3) < 2e-6
+    # Both methods add in single precision in a run-dependent order (float atomics; the tensor
+    # core's partial sums): with ~9000 points on the same cells (clustered) the two sums differ
+    # by about 2e-6 relative from run to run, elsewhere by a few 1e-7.
+    assert oracle.rel_l2(out5, out3) < (4e-6 if case == "clustered" else 2e-6)
 
 
 @pytest.mark.parametrize("sign", [-1, 1])
