@@ -10,7 +10,8 @@
 //  - pass 1 records each point's rank inside its tile (the only atomic);
 //  - a three-kernel device-wide exclusive scan gives tile offsets in tile order;
 //  - pass 2 writes one 32-byte record per point (perm, packed cell, fractions), a full sector,
-//    with no atomics.
+//    with no atomics, as one 256-bit evict-first store where the record array is 32-byte
+//    aligned.
 #include "kernels.cuh"
 
 namespace nnb {
@@ -127,11 +128,15 @@ __global__ void __launch_bounds__(kBinBlock)
 template <typename T, int DIM>
 __global__ void __launch_bounds__(kBinBlock)
     bin_scatter_kernel(BinGeom g, CoordPtrs<T> x, i64 M, const u32* ranks, const u32* bin_start,
-                       PointRec<T>* recs) {
+                       PointRec<T>* recs, bool wide) {
   const i64 stride = i64(gridDim.x) * kBinBlock;
   double inv_tile[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) inv_tile[d] = 1.0 / double(g.tile[d]);
+  // The tile offsets (4 bytes per tile, read at random by every point) stay in the L2; the
+  // records, written once to random slots and read only by the next kernels, leave it first.
+  const unsigned long long keep = l2_evict_last_policy();
+  const unsigned long long pass = l2_evict_first_policy();
   for (i64 base = blockIdx.x * i64(kBinBlock) + threadIdx.x; base < M;
        base += stride * kBinUnroll) {
     T v[kBinUnroll][DIM];
@@ -178,13 +183,16 @@ __global__ void __launch_bounds__(kBinBlock)
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
       if (base + u * stride < M) {
-        pos[u] = NNB_CHECK_INDEX(tile_lin[u], g.total_tiles) ? bin_start[tile_lin[u]] + rank[u]
-                                                             : u32(M);
+        pos[u] = NNB_CHECK_INDEX(tile_lin[u], g.total_tiles)
+                     ? load_u32_policy(bin_start + tile_lin[u], keep) + rank[u]
+                     : u32(M);
       }
     }
 #pragma unroll
     for (int u = 0; u < kBinUnroll; ++u) {
-      if (base + u * stride < M && NNB_CHECK_INDEX(pos[u], M)) store_rec(&recs[pos[u]], r[u]);
+      if (base + u * stride < M && NNB_CHECK_INDEX(pos[u], M)) {
+        store_sector_policy(&recs[pos[u]], rec_sector(r[u]), wide, pass);
+      }
     }
   }
 }
@@ -283,6 +291,10 @@ __global__ void __launch_bounds__(kScanThreads)
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = block_offsets[nb];
 }
 
+// Whether a record array starts on a 32-byte boundary (a user allocator may return less), so
+// that its records take single 256-bit stores.
+bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
+
 int grid_for(i64 n, int block) {
   i64 g = (n + block - 1) / block;
   const i64 cap = 148 * 32;  // grid-stride loops beyond this many blocks
@@ -325,9 +337,9 @@ void launch_bin_scatter(const BinGeom& g, CoordPtrs<T> x, i64 M, const u32* rank
   if (M <= 0) return;
   const int grid = grid_for(M, kBinBlock);
   switch (g.dim) {
-    case 1: bin_scatter_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
-    case 2: bin_scatter_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
-    default: bin_scatter_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec); break;
+    case 1: bin_scatter_kernel<T, 1><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec, aligned32(rec)); break;
+    case 2: bin_scatter_kernel<T, 2><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec, aligned32(rec)); break;
+    default: bin_scatter_kernel<T, 3><<<grid, kBinBlock, 0, stream>>>(g, x, M, ranks, bin_start, rec, aligned32(rec)); break;
   }
   NNB_LAUNCH_CHECK();
 }

@@ -194,27 +194,67 @@ struct alignas(16) PointRec {
 static_assert(sizeof(PointRec<float>) == 32 && sizeof(PointRec<double>) == 32,
               "point records are one 32-byte sector");
 
-// Stores a record as one whole 32-byte sector: two 16-byte stores, the single-precision padding
-// written as zeros. A store of the fields alone leaves part of the sector unwritten, and the L2
-// then reads the sector from memory to merge it when it writes it back: for records placed at
-// random, a second 32 bytes of traffic per point.
-__device__ __forceinline__ void store_rec(PointRec<float>* dst, const PointRec<float>& r) {
-  uint4* d = reinterpret_cast<uint4*>(dst);
-  d[0] = make_uint4(r.perm, r.local, __float_as_uint(r.frac[0]), __float_as_uint(r.frac[1]));
-  d[1] = make_uint4(__float_as_uint(r.frac[2]), 0u, 0u, 0u);
-}
-__device__ __forceinline__ void store_rec(PointRec<double>* dst, const PointRec<double>& r) {
-  uint4* d = reinterpret_cast<uint4*>(dst);
-  d[0] = make_uint4(r.perm, r.local, u32(__double2loint(r.frac[0])),
-                    u32(__double2hiint(r.frac[0])));
-  d[1] = make_uint4(u32(__double2loint(r.frac[1])), u32(__double2hiint(r.frac[1])),
-                    u32(__double2loint(r.frac[2])), u32(__double2hiint(r.frac[2])));
-}
 // The whole sector of a record, as two 16-byte vectors (copies keep the sector whole).
 template <typename T>
 struct RecSector {
   uint4 a, b;
 };
+// The 32 bytes of a record as two 16-byte vectors, the single-precision padding as zeros: a
+// store of the fields alone would leave part of the sector unwritten, and the L2 would read the
+// sector from memory to merge it when it writes it back (for records placed at random, a second
+// 32 bytes of traffic per point).
+__device__ __forceinline__ RecSector<float> rec_sector(const PointRec<float>& r) {
+  return RecSector<float>{make_uint4(r.perm, r.local, __float_as_uint(r.frac[0]),
+                                     __float_as_uint(r.frac[1])),
+                          make_uint4(__float_as_uint(r.frac[2]), 0u, 0u, 0u)};
+}
+__device__ __forceinline__ RecSector<double> rec_sector(const PointRec<double>& r) {
+  return RecSector<double>{
+      make_uint4(r.perm, r.local, u32(__double2loint(r.frac[0])), u32(__double2hiint(r.frac[0]))),
+      make_uint4(u32(__double2loint(r.frac[1])), u32(__double2hiint(r.frac[1])),
+                 u32(__double2loint(r.frac[2])), u32(__double2hiint(r.frac[2])))};
+}
+
+// L2 eviction policies (createpolicy, sm_80 and later) for data that should stay in the L2
+// (evict_last) or leave it first (evict_first).
+__device__ __forceinline__ unsigned long long l2_evict_last_policy() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_evict_first_policy() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// A 32-bit global load with an L2 eviction policy.
+__device__ __forceinline__ u32 load_u32_policy(const u32* p, unsigned long long policy) {
+  u32 v;
+  asm("ld.global.L2::cache_hint.u32 %0, [%1], %2;"
+      : "=r"(v)
+      : "l"(__cvta_generic_to_global(p)), "l"(policy));
+  return v;
+}
+// Stores a record's sector s at dst. Where the record array is 32-byte aligned (`wide`, the same
+// for every thread of a launch; a user allocator may return less) it is one 256-bit store
+// (st.global.v8.b32, sm_100) with the L2 eviction policy `policy`, else two 16-byte stores. The
+// binning scatter, which writes each of 1e8 records to a random slot, takes 4.45 ms with single
+// 256-bit stores and 4.10 ms with single evict-first stores, against 5.71 ms with two 16-byte
+// stores per record.
+template <typename T>
+__device__ __forceinline__ void store_sector_policy(PointRec<T>* dst, const RecSector<T>& s,
+                                                    bool wide, unsigned long long policy) {
+  if (wide) {
+    asm volatile(
+        "st.global.L2::cache_hint.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;"
+        :
+        : "l"(__cvta_generic_to_global(dst)), "r"(s.a.x), "r"(s.a.y), "r"(s.a.z), "r"(s.a.w),
+          "r"(s.b.x), "r"(s.b.y), "r"(s.b.z), "r"(s.b.w), "l"(policy)
+        : "memory");
+  } else {
+    store_sector(dst, s);
+  }
+}
 template <typename T>
 __device__ __forceinline__ RecSector<T> load_sector(const PointRec<T>* src) {
   const uint4* s = reinterpret_cast<const uint4*>(src);

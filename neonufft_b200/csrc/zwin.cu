@@ -130,8 +130,8 @@ struct ZShape {
   // no spills; 86 uncapped, which allows only 5 CTAs and measured 6 % slower), 5 in double.
   static constexpr int INTERP_CTAS = sizeof(T) == 4 ? 6 : 5;
   // CTAs per SM the two-vector spreading kernel is compiled for: a budget of about 88 registers
-  // a thread (7 CTAs of 96 threads; 80 registers, 16 bytes of spills outside the point loop).
-  // Uncapped, the allocator takes 158 registers for w = 8, which leaves 2 CTAs per SM.
+  // a thread (7 CTAs of 96 threads; ptxas then allocates 80 registers and spills 24 bytes for
+  // w = 8). Uncapped, the allocator takes 158 registers for w = 8, which leaves 2 CTAs per SM.
   static constexpr int SPREAD2_CTAS = 65536 / (NT * 88) > 0 ? 65536 / (NT * 88) : 1;
   static_assert(W <= RZ && P1 <= RY, "window smaller than the kernel footprint");
   static_assert(BATCH % NWARP == 0 && BATCH / NWARP <= 32, "staging threads");

@@ -2,11 +2,12 @@
 
 The binning scatter writes each point's 32-byte record to a random slot (bin_start of its tile +
 its rank); with 4.5e6 points the records (144 MB) outgrow the L2, so every record reaches the
-memory on its own, as one whole sector. The checks are the transforms' own: type 1 against FP64
-direct sums on sampled modes, type 2 against FP64 direct sums at sampled points, type 3 against
-FP64 direct sums at sampled targets; for uniform and clustered points, in 1D, 2D and 3D, single
-and double precision, with slab and z-window tiles. A non-finite coordinate in a large set is
-rejected and leaves the plan usable.
+memory on its own, as one whole sector (one 256-bit store); the sets of 2^24 + 4099 points hold
+537 MB of records. The checks are the transforms' own: type 1 against FP64 direct sums on
+sampled modes, type 2 against FP64 direct sums at sampled points, type 3 against FP64 direct
+sums at sampled targets; for uniform and clustered points, in 1D, 2D and 3D, single and double
+precision, with slab and z-window tiles. A non-finite coordinate in a large set is rejected and
+leaves the plan usable.
 """
 import numpy as np
 import pytest
@@ -16,6 +17,7 @@ from gpu_helpers import col_strides, tdtypes
 pytestmark = pytest.mark.gpu
 
 LARGE = 4_500_001  # records larger than the L2 (126 MB)
+HUGE = (1 << 24) + 4099  # 537 MB of records
 MODES = {1: [2000], 2: [96, 80], 3: [40, 36, 32]}
 SAMPLES = 256
 
@@ -52,12 +54,12 @@ def _rel(torch, got, ref):
     return float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
 
 
+@pytest.mark.parametrize("M", [LARGE, HUGE])
 @pytest.mark.parametrize("dist", ["uniform", "clustered"])
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("dim", [1, 2, 3])
-def test_type1_type2_large_point_sets(dim, dtype, dist, cuda, engine):
+def test_type1_type2_large_point_sets(dim, dtype, dist, M, cuda, engine):
     torch = cuda
-    M = LARGE
     rdt, cdt, npc = tdtypes(torch, dtype)
     tol, bound = _tol(dtype)
     rng = np.random.default_rng(10 * dim + (dist == "clustered"))
@@ -114,9 +116,10 @@ def test_spread_methods_large_set(method, cuda, engine):
     plan.close()
 
 
-def test_type3_large_input_set(cuda, engine):
+@pytest.mark.parametrize("M", [LARGE, HUGE])
+def test_type3_large_input_set(M, cuda, engine):
     torch = cuda
-    M, K = LARGE, 2000
+    K = 2000
     rng = np.random.default_rng(21)
     a = [torch.from_numpy(rng.uniform(-2.0, 3.0, M)).cuda().float() for _ in range(3)]
     b = [torch.from_numpy(rng.uniform(-9.0, 7.0, K)).cuda().float() for _ in range(3)]
@@ -135,10 +138,10 @@ def test_type3_large_input_set(cuda, engine):
     plan.close()
 
 
+@pytest.mark.parametrize("M", [LARGE, HUGE])
 @pytest.mark.parametrize("bad", [float("nan"), float("inf")])
-def test_non_finite_point_in_large_set(bad, cuda, engine):
+def test_non_finite_point_in_large_set(bad, M, cuda, engine):
     torch = cuda
-    M = LARGE
     rng = np.random.default_rng(5)
     modes = [32, 32, 32]
     x = [a.float() for a in _points(torch, rng, M, 3, "uniform")]

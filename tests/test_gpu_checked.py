@@ -8,7 +8,8 @@ reference's debug-build sync-and-check after each launch (src/neonufft/gpu/util/
 
 The GPU test runs the small-case parity suites (the reference's type-1/2 and type-3 matrices,
 every spreading method and tile including the tensor-core spreading, the edge cases and the
-batches) in a child process that loads
+batches) and the large-set binning suite (whose records the checked build also checks for being
+a permutation of the points) in a child process that loads
 the checked library, so that any out-of-range index in those kernels fails the run.
 """
 import os
@@ -46,7 +47,8 @@ def test_parity_suites_under_the_checked_build(cuda):
     if not CHECKED.exists():
         pytest.fail("the checked build is missing: python -m neonufft_b200.build --checked")
     suites = ["tests/test_gpu_type12.py", "tests/test_gpu_type3.py", "tests/test_gpu_methods.py",
-              "tests/test_gpu_tcgen05.py", "tests/test_gpu_edges.py", "tests/test_gpu_batch.py"]
+              "tests/test_gpu_tcgen05.py", "tests/test_gpu_edges.py", "tests/test_gpu_batch.py",
+              "tests/test_gpu_binning.py"]
     env = dict(os.environ, NEONUFFT_B200_LIB=str(CHECKED))
     res = subprocess.run([sys.executable, "-m", "pytest", "-m", "gpu", "-x", "-q",
                           "-p", "no:cacheprovider", *suites],
