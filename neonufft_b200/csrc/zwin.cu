@@ -168,7 +168,9 @@ struct alignas(16) ZSlot
     : ZSlotFields<T, W, TX, TY>, ZSlotPad<(sizeof(ZSlotFields<T, W, TX, TY>) / 16) % 2 == 1> {};
 
 // Stages `count` (<= 16) bin-sorted records `recs` into slots[0 .. count), one warp: lanes
-// 0 .. count - 1 load the records (and, for spreading, the strengths); then lane pair
+// 0 .. count - 1 load the records (and, for spreading, the strengths; with `v2_out`, also the
+// second vector's strengths from `in2`, or zeros where in2 is null, into v2_out[0 .. count), so
+// that both gathers are in flight together); then lane pair
 // (2p, 2p + 1) fills point p's slot with the same instruction stream: the even lane kx and the
 // first half of kz, the odd lane ky and the second half, each zeroing half of the contiguous
 // kx / ky arrays first, so all 32 lanes evaluate kernel values.
@@ -176,7 +178,8 @@ template <typename T, int W, int TX, bool SPREAD, int TY = 8>
 __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX, TY>* slots, const PointRec<T>* recs,
                                            int count, const cplx_t<T>* in,
                                            const cplx_t<T>* prephase, T beta, T c, int lane,
-                                           i64 num) {
+                                           i64 num, const cplx_t<T>* in2 = nullptr,
+                                           cplx_t<T>* v2_out = nullptr) {
   using S = ZShape<T, W, TX, TY>;
   using C = cplx_t<T>;
   constexpr unsigned kFull = 0xffffffffu;
@@ -188,10 +191,17 @@ __device__ __forceinline__ void stage_warp(ZSlot<T, W, TX, TY>* slots, const Poi
   if (lane < count) {
     rec = recs[lane];
     if constexpr (SPREAD) {
+      C v2{T(0), T(0)};
       if (NNB_CHECK_INDEX(rec.perm, num)) {
         v = in[rec.perm];
-        if (prephase) v = cmul(v, prephase[rec.perm]);
+        if (in2) v2 = in2[rec.perm];
+        if (prephase) {
+          const C ph = prephase[rec.perm];
+          v = cmul(v, ph);
+          v2 = cmul(v2, ph);
+        }
       }
+      if (v2_out) v2_out[lane] = v2;
     }
   }
   const int p = lane >> 1;
@@ -422,23 +432,12 @@ __device__ __forceinline__ void spread_zwin_item(const SpreadArgs<T>& a, ZChunks
                            a.pts.M)) {
         break;
       }
+      // NV = 2: the second vector's strengths at the same points (zeros when it is missing)
       stage_warp<T, W, TX, true, TY>(slots[k & 1] + th.warp * PW + c0,
                                  a.pts.rec + cta.pbeg + off + th.warp * PW + c0,
                                  min(count - c0, 16), in, a.prephase, a.beta, a.c, th.lane,
-                                 a.pts.M);
-    }
-    if constexpr (NV > 1) {  // the second vector's strengths at the staged points
-      __syncwarp();
-      if (th.lane < count) {
-        const int j = th.warp * PW + th.lane;
-        C v2{T(0), T(0)};
-        const u32 perm = slots[k & 1][j].perm;
-        if (has2 && NNB_CHECK_INDEX(perm, a.pts.M)) {
-          v2 = in[a.in_bdist + perm];
-          if (a.prephase) v2 = cmul(v2, a.prephase[perm]);
-        }
-        sh.v2[k & 1][j] = v2;
-      }
+                                 a.pts.M, NV > 1 && has2 ? in + a.in_bdist : nullptr,
+                                 NV > 1 ? sh.v2[k & 1] + th.warp * PW + c0 : nullptr);
     }
   };
 
