@@ -2,14 +2,15 @@
 """Benchmark of the B200 NUFFT engine (one JSON line on rank 0).
 
 Workload (default ``ns``): 3D type 1, M = 1e8 points i.i.d. uniform in [-pi, pi)^3, complex64
-strengths N(0,1), N = 256^3 modes, tol 1e-6, upsampfac 2 (fine grid 512^3). Synthetic, seeded
-data; no public dataset is involved. One step = set_points (binning) + transform_type_1, so the
+strengths N(0,1), N = 256^3 modes, tol 1e-6. Synthetic, seeded data; no public dataset is
+involved. One step = set_points (binning) + transform_type_1, so the
 metric, NU points per second per transform, is M / step time (set_points included).
 
 Arms of the same run, on the same points and strengths:
-  - the tuned single-precision engine (width 8, 4-row z-window tiles): ``value`` and ``e2e``;
-  - ``plain_fp64``: the engine's plain FP64 path (reference heuristic w = 7, default tiles),
-    the denominator of ``ratio_vs_plain_fp64``;
+  - the tuned single-precision engine (width 8, upsampling 1.875: fine grid 480^3, 4-row
+    z-window tiles): ``value`` and ``e2e``;
+  - ``plain_fp64``: the engine's plain FP64 path (reference heuristic w = 7, upsampling 2: fine
+    grid 512^3, default tiles), the denominator of ``ratio_vs_plain_fp64``;
   - ``reference_gpu_fp64``: the reference's own FP64 GPU plan, compiled from its sources for
     sm_100a (oracle/_ref), when that build is present.
 Every arm's accuracy is the relative l2 error against FP64 direct sums on 1e4 sampled outputs;
@@ -21,7 +22,7 @@ tuner workloads.
 
 Timing: W untimed warm-up steps, then K steps between CUDA events on the plan's stream,
 bracketed by barrier + synchronize, max over ranks. The inputs (north star: coordinates 1.2 GB,
-strengths 0.8 GB, fine grid 1 GiB) exceed the 126 MB L2, so no extra flush is done.
+strengths 0.8 GB, fine grid 0.9 GB) exceed the 126 MB L2, so no extra flush is done.
 
 Multi-GPU: the path does not shard a single transform; ranks run independent replicas
 (weak scaling, no data-path collective) and ``value`` sums the points of all ranks.
@@ -51,7 +52,7 @@ WORKLOADS = {
                tuned_w=8),
     "ns": dict(name="3D type-1, M=1e8 uniform [-pi,pi)^3, N=256^3, tol 1e-6",
                dim=3, M=100_000_000, N=256, tol=1e-6, types=(1,), seed=7, cpu_sample=1_000_000,
-               tuned_w=8, tuned_tile=(4, 4, 1)),
+               tuned_w=8, tuned_tile=(4, 4, 1), tuned_upsampfac=1.875),
     "c4": dict(name="64 uneven 2D/3D type-1 transforms in one batch, M log-uniform [1e4,1e7], "
                     "N per dim in {64,128,256,512} (3D <= 256), half Gaussian blobs (sigma 0.1), tol 1e-6",
                batch=64, tol=1e-6, types=(1,), seed=4, tuned_w=8),
@@ -581,19 +582,20 @@ def run_type3(args, wl):
     return 0
 
 
-def load_traffic(workload, precision, kernel, w, tile):
+def load_traffic(workload, precision, kernel, w, tile, grid):
     """DRAM bytes (read + write) of one launch of `kernel`, as a linear model a*M + b fitted to
-    ncu captures of the same configuration (rows 'workload precision kernel w tile a b' of
+    ncu captures of the same configuration (rows 'workload precision kernel w tile grid a b' of
     profiles/dram_traffic_fit.txt). None when the configuration was not captured."""
     p = ROOT / "profiles" / "dram_traffic_fit.txt"
     if not p.exists():
         return None
-    key = [workload, precision, kernel, str(w), ",".join(str(int(v)) for v in tile)]
+    key = [workload, precision, kernel, str(w), ",".join(str(int(v)) for v in tile),
+           ",".join(str(int(v)) for v in grid)]
     for line in p.read_text().splitlines():
         cells = line.split()
-        if len(cells) >= 7 and not line.lstrip().startswith("#") and cells[:5] == key:
+        if len(cells) >= 8 and not line.lstrip().startswith("#") and cells[:6] == key:
             try:
-                return float(cells[5]), float(cells[6])
+                return float(cells[6]), float(cells[7])
             except ValueError:
                 return None
     return None
@@ -828,7 +830,10 @@ def run_transform(args, wl):
     tuned = args.precision == "f32" and args.n_spread < 0 and args.spread_method == 0
     tile = (tuple(int(v) for v in args.tile.split(",")) if args.tile
             else (wl.get("tuned_tile", (0, 0, 0)) if tuned else (0, 0, 0)))
-    opt = nnb.Options(tol=tol, upsampfac=args.upsampfac, spread_method=args.spread_method,
+    # ... and its upsampling factor (ns: 1.875, a 480^3 fine grid)
+    sigma = (args.upsampfac if args.upsampfac is not None
+             else (wl.get("tuned_upsampfac", 2.0) if tuned else 2.0))
+    opt = nnb.Options(tol=tol, upsampfac=sigma, spread_method=args.spread_method,
                       n_spread=n_spread, tile=tile)
     plan = nnb.Plan(opt, -1, M, loc, modes)
     info = plan.info()
@@ -992,7 +997,8 @@ def run_transform(args, wl):
         else ("spread", spread_ms, "spread_zwin_kernel")
     if info["spread_method"] != 3:
         kname = {"spread": "spread_slab_kernel", "interp": "interp_slab_kernel"}[dom]
-    model = load_traffic(args.workload, args.precision, kname, w, info["tile"][:dim])
+    model = load_traffic(args.workload, args.precision, kname, w, info["tile"][:dim],
+                         info["grid"][:dim])
     traffic = (model[0] * M + model[1]) if model else None
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
@@ -1035,7 +1041,7 @@ def run_transform(args, wl):
             "data": "synthetic (seeded uniform points, N(0,1) strengths and modes)",
             "config": {"workload": wl["name"], "workload_id": args.workload, "M": M, "N": N,
                        "dim": dim, "tol": tol, "types": list(types),
-                       "upsampfac": args.upsampfac, "n_spread": w, "fine_grid": info["grid"][:dim],
+                       "upsampfac": sigma, "n_spread": w, "fine_grid": info["grid"][:dim],
                        "tile": info["tile"][:dim], "method": info["spread_method"],
                        "precision": args.precision,
                        "step": "set_points + " + " + ".join(f"transform_type_{t}" for t in types),
@@ -1098,7 +1104,9 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="plan precision (f64 with --n-spread 0 is the plain FP64 path)")
     ap.add_argument("--streams", type=int, default=8, help="internal streams of a batch (c4)")
-    ap.add_argument("--upsampfac", type=float, default=2.0, help="upsampling factor sigma")
+    ap.add_argument("--upsampfac", type=float, default=None,
+                    help="upsampling factor sigma (default: the workload's tuned factor for the "
+                         "tuned configuration, else 2)")
     ap.add_argument("--tile", default="",
                     help="engine tile shape, e.g. 4,8,1 (default: the workload's tuned tile, "
                          "else the plan's choice)")
