@@ -118,9 +118,11 @@ NNB_API NeonufftError nnb_plan_transform_type_1(NnbPlan plan, const void* in, vo
  * plan transforms one vector per call): strength vector v at in + v * in_bdist, its modes at
  * out + v * out_bdist (elements; out_bdist at least the span of the strided mode box). Single
  * precision on the z-window kernels (spread methods 3 with the default or 4-row tiles) spreads
- * the vectors two at a time, each staged point serving both, and holds two extra fine grids for
- * it; other plans run the transforms one at a time. Same results as `count` calls of
- * nnb_plan_transform_type_1. */
+ * the vectors two at a time, each staged point serving both, into two fine grids of its own
+ * (four when count > 2: the FFTs and deconvolutions of one pair run on an internal stream of
+ * the plan while the next pair spreads; the plan's stream waits for them before the call
+ * returns, so work enqueued on it afterwards sees every output); other plans run the
+ * transforms one at a time. Same results as `count` calls of nnb_plan_transform_type_1. */
 NNB_API NeonufftError nnb_plan_transform_type_1_many(NnbPlan plan, int64_t count, const void* in,
                                                      int64_t in_bdist, void* out,
                                                      int64_t out_bdist,
