@@ -6,7 +6,10 @@ vectors per pass (each staged point and its kernel values serve both); other pla
 transforms one at a time. Either way every output must equal the single transform's (same
 kernels: to 1e-6 relative in single precision, where only the atomic summation order
 differs) and meet the tolerance against the FP64 direct sums, with odd counts (a lone last
-vector), clustered points (work items split over CTAs) and type-3 batches of odd size.
+vector), clustered points (work items split over CTAs) and type-3 batches of odd size. The FFTs
+and deconvolutions of each pair run on an internal stream while the next pair spreads, on two
+alternating sets of grids: counts of 5 and more reuse a set, and work enqueued on the plan's
+stream after the call must see every output.
 """
 import numpy as np
 import pytest
@@ -35,7 +38,7 @@ def _run(engine, torch, dtype, pts, vecs, modes, **opt):
 
 
 @pytest.mark.parametrize("tile", [(0, 0, 0), (4, 4, 1)])
-@pytest.mark.parametrize("count", [2, 3, 4])
+@pytest.mark.parametrize("count", [2, 3, 4, 5, 8])
 @pytest.mark.parametrize("case", ["uniform", "clustered"])
 def test_many_single_precision_pairs(tile, count, case, cuda, engine, oracle):
     rng = np.random.default_rng(100 + count)
@@ -58,6 +61,38 @@ def test_many_single_precision_pairs(tile, count, case, cuda, engine, oracle):
         assert oracle.rel_l2(many[v], singles[v]) < 1e-6
         ref = direct(oracle, 1, -1, pts, vecs[v], modes, "float32")
         assert oracle.rel_l2(many[v], ref) < bound
+
+
+def test_many_outputs_ordered_on_the_plan_stream(cuda, engine, oracle):
+    """The FFTs and deconvolutions of each pair run on the plan's internal stream; work that the
+    caller enqueues on the plan's stream right after the call (no host synchronisation) must see
+    every output."""
+    torch = cuda
+    rng = np.random.default_rng(77)
+    M, modes, count = 400_000, [48, 40, 44], 7
+    nm = int(np.prod(modes))
+    pts = [rng.uniform(-np.pi, np.pi, M) for _ in range(3)]
+    vecs = np.concatenate([rng.standard_normal(M) + 1j * rng.standard_normal(M)
+                           for _ in range(count)]).astype(np.complex64)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        loc = [torch.from_numpy(p.astype(np.float32)).cuda() for p in pts]
+        inp = torch.from_numpy(vecs).cuda()
+        plan = engine.Plan(engine.Options(tol=1e-6, n_spread=8, tile=(4, 4, 1)), -1, M, loc,
+                           modes, stream=s)
+        out = torch.full((count * nm,), float("nan"), dtype=torch.complex64, device="cuda")
+        plan.transform_type_1_many(inp, out, count, col_strides(modes))
+        copy = out.clone()  # enqueued on s behind the call
+        singles = torch.zeros((count, nm), dtype=torch.complex64, device="cuda")
+        for v in range(count):
+            plan.transform_type_1(inp[v * M:(v + 1) * M], singles[v], col_strides(modes))
+    s.synchronize()
+    plan.close()
+    got = copy.cpu().numpy().reshape(count, nm)
+    ref = singles.cpu().numpy()
+    for v in range(count):
+        assert np.all(np.isfinite(got[v]))
+        assert oracle.rel_l2(got[v], ref[v]) < 1e-6
 
 
 @pytest.mark.parametrize("dtype,dim", [("float64", 3), ("float32", 2), ("float64", 2)])
