@@ -140,6 +140,7 @@ public:
     method_ = choose_method(dim, kp_.w, opt.spread_method, is_single<T>());
     for (int d = 0; d < dim; ++d) nf_[d] = fine_grid_size(modes_[d], opt.upsampfac, kp_.w);
     fft_ = std::make_unique<FftGrid<T>>(alloc_, dim, nf_, sign_, stream_);
+    fft_->enable_mode_pruning(modes_);
     for (int d = 0; d < dim; ++d) {
       corr_[d].set_allocator(alloc_);
       upload(corr_[d], deconv_factors(kp_, nf_[d]), stream_);
@@ -168,7 +169,7 @@ public:
     }
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
-      fft_->exec(stream_);
+      fft_->exec_to_modes(fft_->data(), stream_);
     }
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_DECONV);
@@ -237,7 +238,7 @@ public:
         cplx_t<T>* gj = grids + j * cells;
         {
           ScopedStage st(timer_, pipe_.side, NNB_STAGE_FFT);
-          fft_->exec_on(gj, pipe_.side);
+          fft_->exec_to_modes(gj, pipe_.side);
         }
         ScopedStage st(timer_, pipe_.side, NNB_STAGE_DECONV);
         launch_downsample<T>(deconv_args(out_strides), gj, ov + (v + j) * out_bdist,
@@ -261,7 +262,7 @@ public:
     }
     {
       ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
-      fft_->exec(stream_);
+      fft_->exec_from_modes(fft_->data(), stream_);
     }
     if (M > 0) {
       ScopedStage st(timer_, stream_, NNB_STAGE_INTERP);
@@ -292,7 +293,7 @@ public:
     } else {
       launch_upsample<T>(deconv_args(strides), static_cast<const cplx_t<T>*>(in), fft_->data(),
                          stream_);
-      fft_->exec(stream_);
+      fft_->exec_from_modes(fft_->data(), stream_);
     }
     zwin_build_work_list<T>(geom_, points_.view(), stream_);
   }
@@ -300,7 +301,7 @@ public:
   void fused_post(int type, void* out, const i64* strides) override {
     if (type != 1) return;
     check_strides(dim_, modes_, strides);
-    fft_->exec(stream_);
+    fft_->exec_to_modes(fft_->data(), stream_);
     launch_downsample<T>(deconv_args(strides), fft_->data(), static_cast<cplx_t<T>*>(out),
                          stream_);
   }
@@ -492,6 +493,7 @@ public:
     NNB_CUDA(cudaMemsetAsync(spread_grid_.data(), 0,
                              sizeof(cplx_t<T>) * size_t(spread_cells * batch_), stream_));
     fft_ = std::make_unique<FftGrid<T>>(alloc_, dim_, nfft_, sign_, stream_);
+    fft_->enable_mode_pruning(nf1_);  // the spread grid's nf1 modes feed the FFT grid
     for (int d = 0; d < dim_; ++d) upload(corr_[d], deconv_factors(kp_, nfft_[d]), stream_);
     const PhiHatQuad quad = phi_hat_quadrature(kp_);
     if (quad.z.size() > 32) throw_internal("too many quadrature nodes");
@@ -590,7 +592,7 @@ public:
       }
       {
         ScopedStage st(timer_, stream_, NNB_STAGE_FFT);
-        fft_->exec(stream_);
+        fft_->exec_from_modes(fft_->data(), stream_);
       }
       ScopedStage st(timer_, stream_, NNB_STAGE_INTERP);
       InterpArgs<T> a{};

@@ -220,6 +220,90 @@ FftGrid<T>::FftGrid(std::shared_ptr<DeviceAllocator> alloc, int dim, const i64* 
 template <typename T>
 FftGrid<T>::~FftGrid() {
   if (has_plan_) cufftDestroy(plan_);
+  if (plan_yx_) cufftDestroy(plan_yx_);
+  for (cufftHandle p : plan_z_) {
+    if (p) cufftDestroy(p);
+  }
+}
+
+template <typename T>
+void FftGrid<T>::enable_mode_pruning(const i64* modes) {
+  if (dim_ != 3 || pruned_) return;
+  const i64 nx = nf_[0], ny = nf_[1], nz = nf_[2];
+  const i64 lo = (modes[1] + 1) / 2, hi = modes[1] / 2;  // rows [0, lo) and [ny - hi, ny)
+  // (y, x) then z on a fraction f of the rows costs about 1.05 + 0.71 f ms at 480^3 in single
+  // precision against 1.67 ms for the 3D transform: worth it up to three quarters of the rows
+  if (4 * (lo + hi) > 3 * ny || nx * lo > i64(0x7fffffff) || nx * ny > i64(0x7fffffff)) return;
+  const cufftType type = std::is_same<T, float>::value ? CUFFT_C2C : CUFFT_Z2Z;
+  size_t ws_max = work_.size(), ws = 0;
+  NNB_CUFFT(cufftCreate(&plan_yx_));
+  NNB_CUFFT(cufftSetAutoAllocation(plan_yx_, 0));
+  int n2[2] = {int(ny), int(nx)};  // row-major: y slow, x fast
+  NNB_CUFFT(cufftMakePlanMany(plan_yx_, 2, n2, nullptr, 1, int(nx * ny), nullptr, 1,
+                              int(nx * ny), type, int(nz), &ws));
+  ws_max = std::max(ws_max, ws);
+  const i64 r0[2] = {0, ny - hi}, nr[2] = {lo, hi};
+  nblocks_ = 0;
+  for (int k = 0; k < 2; ++k) {
+    if (nr[k] <= 0) continue;
+    // the same shape as the previous block: one plan serves both
+    if (nblocks_ == 1 && nr[k] == rows_[0]) {
+      row0_[1] = r0[k];
+      rows_[1] = nr[k];
+      nblocks_ = 2;
+      continue;
+    }
+    cufftHandle& pz = plan_z_[nblocks_];
+    NNB_CUFFT(cufftCreate(&pz));
+    NNB_CUFFT(cufftSetAutoAllocation(pz, 0));
+    int n1[1] = {int(nz)};
+    int emb[1] = {int(nz)};
+    // lines (x, y) of the block are consecutive elements; their z elements nx ny apart
+    NNB_CUFFT(cufftMakePlanMany(pz, 1, n1, emb, int(nx * ny), 1, emb, int(nx * ny), 1, type,
+                                int(nx * nr[k]), &ws));
+    ws_max = std::max(ws_max, ws);
+    row0_[nblocks_] = r0[k];
+    rows_[nblocks_] = nr[k];
+    ++nblocks_;
+  }
+  work_.reserve(ws_max);
+  NNB_CUFFT(cufftSetWorkArea(plan_, work_.data()));
+  NNB_CUFFT(cufftSetWorkArea(plan_yx_, work_.data()));
+  for (cufftHandle p : plan_z_) {
+    if (p) NNB_CUFFT(cufftSetWorkArea(p, work_.data()));
+  }
+  pruned_ = true;
+}
+
+template <typename T>
+void FftGrid<T>::exec_plan(cufftHandle plan, cplx_t<T>* data, cudaStream_t stream) {
+  NNB_CUFFT(cufftSetStream(plan, stream));
+  const int dir = sign_ < 0 ? CUFFT_FORWARD : CUFFT_INVERSE;
+  if constexpr (std::is_same<T, float>::value) {
+    NNB_CUFFT(cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(data),
+                           reinterpret_cast<cufftComplex*>(data), dir));
+  } else {
+    NNB_CUFFT(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(data),
+                           reinterpret_cast<cufftDoubleComplex*>(data), dir));
+  }
+}
+
+template <typename T>
+void FftGrid<T>::exec_to_modes(cplx_t<T>* data, cudaStream_t stream) {
+  if (!pruned_) return exec_on(data, stream);
+  exec_plan(plan_yx_, data, stream);
+  for (int k = 0; k < nblocks_; ++k) {
+    exec_plan(plan_z_[k < 2 && plan_z_[k] ? k : 0], data + row0_[k] * nf_[0], stream);
+  }
+}
+
+template <typename T>
+void FftGrid<T>::exec_from_modes(cplx_t<T>* data, cudaStream_t stream) {
+  if (!pruned_) return exec_on(data, stream);
+  for (int k = 0; k < nblocks_; ++k) {
+    exec_plan(plan_z_[k < 2 && plan_z_[k] ? k : 0], data + row0_[k] * nf_[0], stream);
+  }
+  exec_plan(plan_yx_, data, stream);
 }
 
 template <typename T>

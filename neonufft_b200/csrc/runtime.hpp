@@ -130,11 +130,20 @@ public:
   // The same in-place transform on another buffer of the grid's shape (the plan's work area is
   // shared: executions on one stream are ordered).
   void exec_on(cplx_t<T>* data, cudaStream_t stream);
+  // 3D grids that hold (or feed) `modes` modes, stored k mod nf: only the first ceil(n/2) and
+  // the last floor(n/2) rows in y (n = modes[1]) carry modes. Type 1 (exec_to_modes) then needs
+  // the z transform only on those rows, after the (y, x) transforms of every plane; type 2
+  // (exec_from_modes: every other row is zero) needs it before them. Without pruning (other
+  // dimensions, or rows that cover most of the grid) both are the full transform.
+  void enable_mode_pruning(const i64* modes);
+  void exec_to_modes(cplx_t<T>* data, cudaStream_t stream);
+  void exec_from_modes(cplx_t<T>* data, cudaStream_t stream);
   cplx_t<T>* data() const { return grid_.data(); }
   i64 cells() const { return cells_; }
   const i64* nf() const { return nf_; }
 
 private:
+  void exec_plan(cufftHandle plan, cplx_t<T>* data, cudaStream_t stream);
   DevArray<cplx_t<T>> grid_;
   DevArray<unsigned char> work_;
   cufftHandle plan_ = 0;
@@ -143,6 +152,12 @@ private:
   int sign_;
   i64 nf_[3] = {1, 1, 1};
   i64 cells_ = 1;
+  // pruned form: (y, x) transforms of every z plane, and z transforms of the rows
+  // [row0_[k], row0_[k] + rows_[k]) for k < nblocks_
+  cufftHandle plan_yx_ = 0, plan_z_[2] = {0, 0};
+  bool pruned_ = false;
+  int nblocks_ = 0;
+  i64 row0_[2] = {0, 0}, rows_[2] = {0, 0};
 };
 
 // Bin-sorted point set on one fine grid (see binning.cu).
